@@ -1,0 +1,184 @@
+"""CPU oracle for RecSplit construction — TEST INFRASTRUCTURE ONLY.
+
+A scalar C++ restatement of ByteHamster/GpuRecSplit's SIMDRecSplit construction
+(``oracle/recsplit_oracle.cpp``), loaded through ctypes. Only ``tests/``, ``bench.py``
+(its ``cpu_baseline`` leg and ``--impl reference`` arm) and ``__graft_entry__.smoke()``
+may import this module, and only as the checker or the timed CPU baseline; the
+``gpurecsplit_b200`` product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+STATUS = {0: "OK", 1: "BAD_ARG", 2: "DUPLICATE_KEY", 3: "BUCKET_TOO_LARGE", 4: "FORMAT"}
+
+
+def build() -> str:
+    """Compiles the oracle library with the committed Makefile (no-op when up to date)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        u64p = ctypes.POINTER(ctypes.c_uint64)
+        L.orc_memo.argtypes = [ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_build.restype = ctypes.c_void_p
+        L.orc_build.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64,
+                                ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        L.orc_build_buckets.restype = ctypes.c_void_p
+        L.orc_build_buckets.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64,
+                                        ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64,
+                                        ctypes.POINTER(ctypes.c_int)]
+        L.orc_result_len.restype = ctypes.c_uint64
+        L.orc_result_len.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_result_copy.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        L.orc_free.argtypes = [ctypes.c_void_p]
+        L.orc_query.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p,
+                                ctypes.c_uint64, ctypes.c_void_p]
+        L.orc_get_bits.restype = ctypes.c_uint64
+        L.orc_get_bits.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64]
+        L.orc_keygen_hash128.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p]
+        L.orc_keygen_u64.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p]
+        L.orc_hash_u64.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]
+        L.orc_keygen_strings.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
+                                         ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_hash_strings.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]
+        L.orc_remap16.restype = ctypes.c_uint32
+        L.orc_remap16.argtypes = [ctypes.c_uint64, ctypes.c_uint32]
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class OracleError(RuntimeError):
+    def __init__(self, status: int):
+        super().__init__(f"oracle status {status} ({STATUS.get(status, '?')})")
+        self.status = status
+
+
+def memo(leaf: int):
+    out = np.zeros(3000, dtype=np.uint32)
+    lo, up = ctypes.c_uint32(), ctypes.c_uint32()
+    st = lib().orc_memo(leaf, _ptr(out), ctypes.byref(lo), ctypes.byref(up))
+    if st:
+        raise OracleError(st)
+    return out, lo.value, up.value
+
+
+class Build:
+    """Result of one oracle build: serialized bytes, DFS seeds, node sizes, EF inputs."""
+
+    def __init__(self, handle):
+        L = lib()
+        self.bytes = self._get(handle, 0, np.uint8)
+        self.seeds = self._get(handle, 1, np.uint64)
+        self.sizes = self._get(handle, 2, np.uint32)
+        self.bucket_size_acc = self._get(handle, 3, np.uint64)
+        self.bucket_pos_acc = self._get(handle, 4, np.uint64)
+        self.evals_alg = int(self._get(handle, 5, np.uint64)[0])
+        L.orc_free(handle)
+
+    @staticmethod
+    def _get(handle, which, dtype):
+        L = lib()
+        n = L.orc_result_len(handle, which)
+        a = np.zeros(n, dtype=dtype)
+        if n:
+            L.orc_result_copy(handle, which, _ptr(a))
+        return a
+
+
+def build_mphf(keys128: np.ndarray, leaf: int, bucket_size: int, rotate: bool = True, threads: int = 0) -> Build:
+    """keys128: uint64 array of shape (n, 2) holding (first, second)."""
+    keys128 = np.ascontiguousarray(keys128, dtype=np.uint64).reshape(-1, 2)
+    threads = threads or os.cpu_count() or 1
+    st = ctypes.c_int(0)
+    h = lib().orc_build(_ptr(keys128), keys128.shape[0], leaf, bucket_size, int(rotate), threads, ctypes.byref(st))
+    if not h:
+        raise OracleError(st.value)
+    return Build(h)
+
+
+def bucket_seeds(keys128: np.ndarray, leaf: int, bucket_size: int, buckets, rotate: bool = True,
+                 threads: int = 0) -> Build:
+    """Seeds (DFS order) of the selected buckets only; nothing is encoded."""
+    keys128 = np.ascontiguousarray(keys128, dtype=np.uint64).reshape(-1, 2)
+    sel = np.ascontiguousarray(buckets, dtype=np.uint64)
+    threads = threads or os.cpu_count() or 1
+    st = ctypes.c_int(0)
+    h = lib().orc_build_buckets(_ptr(keys128), keys128.shape[0], leaf, bucket_size, int(rotate), threads,
+                                _ptr(sel), sel.size, ctypes.byref(st))
+    if not h:
+        raise OracleError(st.value)
+    return Build(h)
+
+
+def query(serialized: np.ndarray, keys128: np.ndarray, rotate: bool = True) -> np.ndarray:
+    serialized = np.ascontiguousarray(serialized, dtype=np.uint8)
+    keys128 = np.ascontiguousarray(keys128, dtype=np.uint64).reshape(-1, 2)
+    out = np.zeros(keys128.shape[0], dtype=np.uint64)
+    st = lib().orc_query(_ptr(serialized), serialized.size, int(rotate), _ptr(keys128), keys128.shape[0], _ptr(out))
+    if st:
+        raise OracleError(st)
+    return out
+
+
+def get_bits(serialized: np.ndarray, object_bytes: int = 0) -> int:
+    serialized = np.ascontiguousarray(serialized, dtype=np.uint8)
+    return int(lib().orc_get_bits(_ptr(serialized), serialized.size, object_bytes))
+
+
+def keygen_hash128(seed: int, n: int) -> np.ndarray:
+    out = np.zeros((n, 2), dtype=np.uint64)
+    lib().orc_keygen_hash128(seed, n, _ptr(out))
+    return out
+
+
+def keygen_u64(seed: int, n: int) -> np.ndarray:
+    out = np.zeros(n, dtype=np.uint64)
+    lib().orc_keygen_u64(seed, n, _ptr(out))
+    return out
+
+
+def hash_u64(keys: np.ndarray) -> np.ndarray:
+    keys = np.ascontiguousarray(keys, dtype=np.uint64)
+    out = np.zeros((keys.size, 2), dtype=np.uint64)
+    lib().orc_hash_u64(_ptr(keys), keys.size, _ptr(out))
+    return out
+
+
+def keygen_strings(seed: int, n: int, min_len: int = 10, max_len: int = 50):
+    offsets = np.zeros(n + 1, dtype=np.uint64)
+    lib().orc_keygen_strings(seed, n, min_len, max_len, _ptr(offsets), None)
+    data = np.zeros(int(offsets[-1]), dtype=np.uint8)
+    lib().orc_keygen_strings(seed, n, min_len, max_len, _ptr(offsets), _ptr(data))
+    return data, offsets
+
+
+def hash_strings(data: np.ndarray, offsets: np.ndarray) -> np.ndarray:
+    data = np.ascontiguousarray(data, dtype=np.uint8)
+    offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+    n = offsets.size - 1
+    out = np.zeros((n, 2), dtype=np.uint64)
+    lib().orc_hash_strings(_ptr(data), _ptr(offsets), n, _ptr(out))
+    return out
+
+
+def remap16(x: int, n: int) -> int:
+    return int(lib().orc_remap16(x, n))
