@@ -1,0 +1,337 @@
+"""B200-native RecSplit construction engine (Python binding of librsb.so).
+
+Mirrors the construction API of ByteHamster/GpuRecSplit
+(``GPURecSplit<LEAF_SIZE, AT, USE_BIJECTIONS_ROTATE>``, include/function/GPURecSplit.cuh:409-505):
+
+    f = GPURecSplit(keys, bucket_size=2000, leaf_size=16)   # keys: hash128 array, strings or bytes
+    f(key)                                                   # operator()
+    f.get_bits()                                             # getBits()
+    blob = f.serialize(); g = GPURecSplit.deserialize(blob, leaf_size=16)   # operator<< / >>
+
+All construction runs in CUDA kernels for sm_100a through the C ABI of ``include/rsb.h``.
+There is no CPU fallback: without the built library or a B200 every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Iterable, Optional, Sequence, Union
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "librsb.so")
+
+RSB_ROTATE = 1
+RSB_KEYS_ON_DEVICE = 2
+RSB_DEVICE_ONLY = 4
+RSB_KEEP_SEEDS = 8
+
+STATUS_NAMES = {
+    0: "OK", 1: "BAD_ARG", 2: "CUDA", 3: "OOM", 4: "DUPLICATE_KEY", 5: "SEARCH_BUDGET",
+    6: "BUCKET_TOO_LARGE", 7: "TIMEOUT", 8: "FORMAT", 9: "INTERNAL", 10: "NO_DEVICE",
+}
+
+_lib = None
+
+
+class RSBError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        msg = lib().rsb_strerror(status).decode()
+        super().__init__(f"{what}: rsb status {status} ({STATUS_NAMES.get(status, '?')}): {msg}")
+        self.status = status
+        self.name = STATUS_NAMES.get(status, "?")
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("keys", ctypes.c_uint64), ("buckets", ctypes.c_uint64), ("nodes", ctypes.c_uint64),
+        ("nodes_per_stage", ctypes.c_uint64 * 21), ("evals_alg", ctypes.c_uint64),
+        ("descriptor_bits", ctypes.c_uint64), ("ms_total", ctypes.c_double), ("ms_partition", ctypes.c_double),
+        ("ms_search", ctypes.c_double * 21), ("ms_encode", ctypes.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {
+            "keys": self.keys, "buckets": self.buckets, "nodes": self.nodes,
+            "nodes_per_stage": list(self.nodes_per_stage), "evals_alg": self.evals_alg,
+            "descriptor_bits": self.descriptor_bits, "ms_total": self.ms_total,
+            "ms_partition": self.ms_partition, "ms_search": list(self.ms_search), "ms_encode": self.ms_encode,
+        }
+
+
+def build_library() -> str:
+    from . import build as _build
+    return _build.build()
+
+
+def lib():
+    """Loads librsb.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run `python -m gpurecsplit_b200.build` first")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, u64, u32, i32 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int
+        pp = ctypes.POINTER(ctypes.c_void_p)
+        sig = {
+            "rsb_engine_create": ([i32, vp, pp], i32),
+            "rsb_engine_destroy": ([vp], i32),
+            "rsb_engine_set_budget": ([vp, u32, u64], i32),
+            "rsb_build_hash128": ([vp, vp, u64, u64, u32, u32, pp], i32),
+            "rsb_build_strings": ([vp, vp, vp, u64, u64, u32, u32, pp], i32),
+            "rsb_build_u64": ([vp, vp, u64, u64, u32, u32, pp], i32),
+            "rsb_query_hash128": ([vp, vp, u64, vp], i32),
+            "rsb_query_strings": ([vp, vp, vp, u64, vp], i32),
+            "rsb_query_device": ([vp, vp, vp, u64, vp], i32),
+            "rsb_get_bits": ([vp, ctypes.POINTER(u64)], i32),
+            "rsb_serialize": ([vp, vp, ctypes.POINTER(ctypes.c_size_t)], i32),
+            "rsb_deserialize": ([vp, ctypes.c_size_t, u32, u32, pp], i32),
+            "rsb_seeds": ([vp, vp, vp, ctypes.POINTER(ctypes.c_size_t)], i32),
+            "rsb_get_stats": ([vp, ctypes.POINTER(Stats)], i32),
+            "rsb_free": ([vp], i32),
+            "rsb_hash_strings": ([vp, vp, vp, u64, u32, vp], i32),
+            "rsb_hash_u64": ([vp, vp, u64, u32, vp], i32),
+            "rsb_strerror": ([i32], ctypes.c_char_p),
+            "rsb_version": ([], ctypes.c_char_p),
+            "rsb_golomb_memo": ([u32, vp], i32),
+        }
+        for name, (args, res) in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def _check(status: int, what: str) -> None:
+    if status != 0:
+        raise RSBError(status, what)
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def golomb_memo(leaf_size: int) -> np.ndarray:
+    """The engine's Golomb-Rice table (AbstractParallelRecSplit.hpp:191-227) for one leaf size."""
+    out = np.zeros(3000, dtype=np.uint32)
+    _check(lib().rsb_golomb_memo(leaf_size, _ptr(out)), "rsb_golomb_memo")
+    return out
+
+
+class Engine:
+    """A device context (stream + cached scratch); one per GPU and host thread."""
+
+    def __init__(self, device: int = 0, stream: Optional[int] = None):
+        h = ctypes.c_void_p()
+        _check(lib().rsb_engine_create(device, ctypes.c_void_p(stream or 0), ctypes.byref(h)), "rsb_engine_create")
+        self._h = h
+        self.device = device
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_budget(self, shift: int, min_candidates: int = 1 << 16) -> None:
+        _check(lib().rsb_engine_set_budget(self._h, shift, min_candidates), "rsb_engine_set_budget")
+
+    def close(self) -> None:
+        if self._h:
+            lib().rsb_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_engines: dict = {}
+
+
+def default_engine(device: int = 0) -> Engine:
+    e = _default_engines.get(device)
+    if e is None:
+        e = Engine(device)
+        _default_engines[device] = e
+    return e
+
+
+def _strings_to_arrays(keys: Sequence[Union[str, bytes]]):
+    bs = [k.encode() if isinstance(k, str) else bytes(k) for k in keys]
+    offsets = np.zeros(len(bs) + 1, dtype=np.uint64)
+    if bs:
+        offsets[1:] = np.cumsum([len(b) for b in bs], dtype=np.uint64)
+    data = np.frombuffer(b"".join(bs), dtype=np.uint8) if bs else np.zeros(0, dtype=np.uint8)
+    return np.ascontiguousarray(data), offsets
+
+
+class GPURecSplit:
+    """Minimal perfect hash function built on the GPU (drop-in for the reference class).
+
+    ``keys`` may be a uint64 array of shape (n, 2) holding hash128 (first, second) pairs,
+    a sequence of str/bytes (hashed with SpookyHash V2 like the reference's string
+    constructor), or — with ``key_type="u64"`` — a uint64 array of 64-bit keys.
+    """
+
+    def __init__(self, keys=None, bucket_size: int = 100, leaf_size: int = 8, rotate: bool = True,
+                 engine: Optional[Engine] = None, key_type: Optional[str] = None, keep_seeds: bool = False,
+                 device_only: bool = False, _handle=None):
+        self.leaf_size = leaf_size
+        self.bucket_size = bucket_size
+        self.rotate = rotate
+        self._h = _handle
+        if _handle is not None:
+            return
+        eng = engine or default_engine()
+        flags = (RSB_ROTATE if rotate else 0) | (RSB_KEEP_SEEDS if keep_seeds else 0) | (RSB_DEVICE_ONLY if device_only else 0)
+        h = ctypes.c_void_p()
+        L = lib()
+        if key_type is None:
+            if isinstance(keys, np.ndarray):
+                key_type = "hash128" if keys.ndim == 2 else "u64"
+            else:
+                key_type = "strings"
+        if key_type == "hash128":
+            k = np.ascontiguousarray(keys, dtype=np.uint64).reshape(-1, 2)
+            st = L.rsb_build_hash128(eng.handle, _ptr(k), k.shape[0], bucket_size, leaf_size, flags, ctypes.byref(h))
+        elif key_type == "u64":
+            k = np.ascontiguousarray(keys, dtype=np.uint64).reshape(-1)
+            st = L.rsb_build_u64(eng.handle, _ptr(k), k.size, bucket_size, leaf_size, flags, ctypes.byref(h))
+        elif key_type == "strings":
+            if isinstance(keys, tuple) and len(keys) == 2 and isinstance(keys[0], np.ndarray):
+                data, offsets = keys
+            else:
+                data, offsets = _strings_to_arrays(keys)
+            data = np.ascontiguousarray(data, dtype=np.uint8)
+            offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+            st = L.rsb_build_strings(eng.handle, _ptr(data), _ptr(offsets), offsets.size - 1, bucket_size, leaf_size,
+                                     flags, ctypes.byref(h))
+        else:
+            raise ValueError(f"unknown key_type {key_type!r}")
+        _check(st, "build")
+        self._h = h
+
+    # ---- device-resident construction (torch CUDA tensors or raw device pointers) ----
+    @classmethod
+    def from_device(cls, keys_ptr: int, n: int, bucket_size: int, leaf_size: int, rotate: bool = True,
+                    key_type: str = "hash128", engine: Optional[Engine] = None, device_only: bool = True,
+                    keep_seeds: bool = False) -> "GPURecSplit":
+        eng = engine or default_engine()
+        flags = RSB_KEYS_ON_DEVICE | (RSB_ROTATE if rotate else 0) | (RSB_DEVICE_ONLY if device_only else 0) | \
+            (RSB_KEEP_SEEDS if keep_seeds else 0)
+        h = ctypes.c_void_p()
+        L = lib()
+        if key_type == "hash128":
+            st = L.rsb_build_hash128(eng.handle, ctypes.c_void_p(keys_ptr), n, bucket_size, leaf_size, flags, ctypes.byref(h))
+        elif key_type == "u64":
+            st = L.rsb_build_u64(eng.handle, ctypes.c_void_p(keys_ptr), n, bucket_size, leaf_size, flags, ctypes.byref(h))
+        else:
+            raise ValueError(key_type)
+        _check(st, "build (device keys)")
+        return cls(bucket_size=bucket_size, leaf_size=leaf_size, rotate=rotate, _handle=h)
+
+    # ---- queries ----
+    def __call__(self, key) -> int:
+        if isinstance(key, (str, bytes)):
+            return int(self.query_strings([key])[0])
+        k = np.asarray(key, dtype=np.uint64).reshape(1, 2)
+        return int(self.query(k)[0])
+
+    def query(self, keys128: np.ndarray) -> np.ndarray:
+        k = np.ascontiguousarray(keys128, dtype=np.uint64).reshape(-1, 2)
+        out = np.zeros(k.shape[0], dtype=np.uint64)
+        _check(lib().rsb_query_hash128(self._h, _ptr(k), k.shape[0], _ptr(out)), "query")
+        return out
+
+    def query_strings(self, keys) -> np.ndarray:
+        if isinstance(keys, tuple) and len(keys) == 2 and isinstance(keys[0], np.ndarray):
+            data, offsets = keys
+        else:
+            data, offsets = _strings_to_arrays(keys)
+        data = np.ascontiguousarray(data, dtype=np.uint8)
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+        out = np.zeros(offsets.size - 1, dtype=np.uint64)
+        _check(lib().rsb_query_strings(self._h, _ptr(data), _ptr(offsets), offsets.size - 1, _ptr(out)), "query_strings")
+        return out
+
+    def query_device(self, keys_ptr: int, n: int, out_ptr: int, engine: Optional[Engine] = None) -> None:
+        eng = engine or default_engine()
+        _check(lib().rsb_query_device(eng.handle, self._h, ctypes.c_void_p(keys_ptr), n, ctypes.c_void_p(out_ptr)),
+               "query_device")
+
+    # ---- accessors ----
+    def get_bits(self, object_bytes: int = 0) -> int:
+        b = ctypes.c_uint64()
+        _check(lib().rsb_get_bits(self._h, ctypes.byref(b)), "get_bits")
+        return b.value + 8 * object_bytes
+
+    def serialize(self) -> bytes:
+        n = ctypes.c_size_t(0)
+        _check(lib().rsb_serialize(self._h, None, ctypes.byref(n)), "serialize")
+        buf = np.zeros(n.value, dtype=np.uint8)
+        _check(lib().rsb_serialize(self._h, _ptr(buf), ctypes.byref(n)), "serialize")
+        return buf[: n.value].tobytes()
+
+    @classmethod
+    def deserialize(cls, blob: bytes, leaf_size: int, rotate: bool = True) -> "GPURecSplit":
+        b = np.frombuffer(blob, dtype=np.uint8).copy()
+        h = ctypes.c_void_p()
+        _check(lib().rsb_deserialize(_ptr(b), b.size, leaf_size, RSB_ROTATE if rotate else 0, ctypes.byref(h)),
+               "deserialize")
+        return cls(leaf_size=leaf_size, rotate=rotate, _handle=h)
+
+    def seeds(self):
+        n = ctypes.c_size_t(0)
+        _check(lib().rsb_seeds(self._h, None, None, ctypes.byref(n)), "seeds")
+        s = np.zeros(n.value, dtype=np.uint64)
+        z = np.zeros(n.value, dtype=np.uint32)
+        if n.value:
+            _check(lib().rsb_seeds(self._h, _ptr(s), _ptr(z), ctypes.byref(n)), "seeds")
+        return s, z
+
+    def stats(self) -> dict:
+        s = Stats()
+        _check(lib().rsb_get_stats(self._h, ctypes.byref(s)), "stats")
+        return s.as_dict()
+
+    def close(self) -> None:
+        if self._h:
+            lib().rsb_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def hash_strings(keys, engine: Optional[Engine] = None) -> np.ndarray:
+    """Device SpookyHash V2 of string keys -> (n, 2) uint64 (first, second)."""
+    eng = engine or default_engine()
+    if isinstance(keys, tuple) and len(keys) == 2 and isinstance(keys[0], np.ndarray):
+        data, offsets = keys
+    else:
+        data, offsets = _strings_to_arrays(keys)
+    data = np.ascontiguousarray(data, dtype=np.uint8)
+    offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+    n = offsets.size - 1
+    out = np.zeros((n, 2), dtype=np.uint64)
+    _check(lib().rsb_hash_strings(eng.handle, _ptr(data), _ptr(offsets), n, 0, _ptr(out)), "hash_strings")
+    return out
+
+
+def hash_u64(keys: np.ndarray, engine: Optional[Engine] = None) -> np.ndarray:
+    """Device 64->128-bit key mixer -> (n, 2) uint64 (first, second)."""
+    eng = engine or default_engine()
+    k = np.ascontiguousarray(keys, dtype=np.uint64).reshape(-1)
+    out = np.zeros((k.size, 2), dtype=np.uint64)
+    _check(lib().rsb_hash_u64(eng.handle, _ptr(k), k.size, 0, _ptr(out)), "hash_u64")
+    return out
+
+
+__all__ = ["GPURecSplit", "Engine", "RSBError", "lib", "build_library", "golomb_memo", "hash_strings", "hash_u64",
+           "default_engine", "LIB_PATH"]

@@ -1,0 +1,851 @@
+// C ABI of the construction engine: engine lifetime, the device build pipeline, handles,
+// serialization and host/device queries. See include/rsb.h for the contract of each call.
+//
+// Build pipeline (one CUDA stream, no host synchronisation until the end):
+//   keys -> hash128 -> bucket histogram -> scan -> scatter -> per-bucket sort/dup check
+//   -> node counts -> scan -> tree emission -> stage lists
+//   -> fanout-2 depths (CTA per node) -> upper aggr -> partition -> lower aggr -> partition
+//   -> rotation leaves -> brute-force leaves
+//   -> bucket bit lengths -> scan -> Rice writer + sentinel -> double Elias-Fano
+// It replaces GPURecSplit::hash_gen (GPURecSplit.cuh:637-815), which runs the sort,
+// grouping, unpacking and encoding on the host and calls cudaDeviceReset at the end.
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "rsb_kernels.cuh"
+#include "rsb_query.cuh"
+#include "rsb_spooky.cuh"
+#include "rsb_tables.h"
+
+using namespace rsb;
+
+namespace {
+
+thread_local cudaError_t g_last_cuda = cudaSuccess;
+
+#define RSB_CK(call)                           \
+    do {                                       \
+        cudaError_t e_ = (call);               \
+        if (e_ != cudaSuccess) {               \
+            g_last_cuda = e_;                  \
+            return RSB_ERR_CUDA;               \
+        }                                      \
+    } while (0)
+
+template <typename T>
+struct DBuf {
+    T *p = nullptr;
+    size_t cap = 0;
+};
+
+template <typename T>
+rsb_status ensure(DBuf<T> &b, size_t n) {
+    if (n == 0) n = 1;
+    if (b.p && n <= b.cap) return RSB_OK;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    const size_t want = n + n / 8;  // headroom against frequent regrowth
+    cudaError_t e = cudaMalloc((void **)&b.p, want * sizeof(T));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        b.p = nullptr;
+        return RSB_ERR_OOM;
+    }
+    b.cap = want;
+    return RSB_OK;
+}
+
+template <typename T>
+void release(DBuf<T> &b) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+}
+
+constexpr int kNumEvents = 6 + kNumStages;  // start, hashed/partitioned, stage boundaries, encoded
+
+}  // namespace
+
+struct rsb_engine {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int num_sms = 0;
+    uint32_t budget_shift = 10;
+    uint64_t budget_min = 1ull << 16;
+    std::map<uint32_t, std::pair<uint32_t *, uint32_t *>> tables;  // (leaf, rotate) -> device memo, nodes
+    DBuf<uint64_t> keys128, raw_u64, offsets, sorted, acc, node_base, scan_tmp, pos_acc, seed;
+    DBuf<uint32_t> counts, node_count, lists, stage_info, sched, slots, bits, fixed_bits, nstart, nwin;
+    DBuf<uint16_t> nsize;
+    DBuf<uint8_t> nstage, bytes;
+    DBuf<DevStatus> status;
+    DBuf<EfParams> efp;
+    cudaEvent_t ev[kNumEvents] = {};
+};
+
+struct rsb_mphf {
+    uint32_t leaf = 0;
+    bool rotate = true;
+    uint64_t bucket_size = 0, keys_count = 0, nbuckets = 0;
+    EfParams ef{};
+    int device = -1;
+    uint64_t *d_block = nullptr;  // desc | lower | upper_cum | upper_pos | jump (device copy)
+    uint64_t desc_cap = 0, lower_cap = 0, cum_cap = 0, pos_cap = 0, jump_cap = 0;
+    bool host_valid = false;
+    std::vector<uint64_t> desc, lower, upper_cum, upper_pos, jump;
+    std::vector<uint64_t> seeds;
+    std::vector<uint32_t> sizes;
+    rsb_stats stats{};
+    const LeafTables *tab = nullptr;
+
+    uint64_t *d_desc() const { return d_block; }
+    uint64_t *d_lower() const { return d_block + desc_cap; }
+    uint64_t *d_cum() const { return d_lower() + lower_cap; }
+    uint64_t *d_pos() const { return d_cum() + cum_cap; }
+    uint64_t *d_jump() const { return d_pos() + pos_cap; }
+
+    MphfView host_view() const {
+        MphfView v{};
+        v.sh = tab->shape;
+        v.nbuckets = nbuckets;
+        v.desc = desc.data();
+        v.desc_words = desc.size();
+        v.u_cum_keys = ef.u_cum_keys;
+        v.u_position = ef.u_position;
+        v.l_cum_keys = ef.l_cum_keys;
+        v.l_position = ef.l_position;
+        v.cum_keys_min_delta = ef.cum_keys_min_delta;
+        v.min_diff = ef.min_diff;
+        v.bits_per_key_fixed_point = ef.bits_per_key_fixed_point;
+        v.lower = lower.data();
+        v.upper_cum = upper_cum.data();
+        v.upper_pos = upper_pos.data();
+        v.jump = jump.data();
+        v.lower_words = lower.size();
+        v.cum_words = upper_cum.size();
+        v.pos_words = upper_pos.size();
+        v.jump_words = jump.size();
+        v.memo = tab->memo.data();
+        return v;
+    }
+};
+
+namespace {
+
+rsb_status get_device_tables(rsb_engine *e, const LeafTables &t, uint32_t leaf, bool rotate, DevTables &out) {
+    const uint32_t key = leaf * 2 + (rotate ? 1 : 0);
+    auto it = e->tables.find(key);
+    if (it == e->tables.end()) {
+        uint32_t *d = nullptr;
+        if (cudaMalloc((void **)&d, 2 * kMaxBucketSize * sizeof(uint32_t)) != cudaSuccess) {
+            cudaGetLastError();
+            return RSB_ERR_OOM;
+        }
+        RSB_CK(cudaMemcpy(d, t.memo.data(), kMaxBucketSize * sizeof(uint32_t), cudaMemcpyHostToDevice));
+        RSB_CK(cudaMemcpy(d + kMaxBucketSize, t.nodes.data(), kMaxBucketSize * sizeof(uint32_t), cudaMemcpyHostToDevice));
+        it = e->tables.emplace(key, std::make_pair(d, d + kMaxBucketSize)).first;
+    }
+    out.memo = it->second.first;
+    out.nodes = it->second.second;
+    return RSB_OK;
+}
+
+bool is_device_pointer(const void *p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return ms;
+}
+
+uint64_t jump_words_for(uint64_t nb) {
+    constexpr uint64_t q = 256, super_q = 1 << 14, sqs = 1 + (super_q / q) / 4;
+    uint64_t jw = (nb / super_q) * sqs * 2;
+    if (nb % super_q != 0) jw += (1 + ((nb % super_q + q - 1) / q + 3) / 4) * 2;
+    return jw;
+}
+
+rsb_status copy_to_host(rsb_mphf *h, cudaStream_t st) {
+    if (h->host_valid) return RSB_OK;
+    if (!h->d_block) return RSB_ERR_INTERNAL;
+    h->desc.resize(h->ef.desc_words);
+    h->lower.resize(h->ef.lower_words);
+    h->upper_cum.resize(h->ef.cum_words);
+    h->upper_pos.resize(h->ef.pos_words);
+    h->jump.resize(h->ef.jump_words);
+    RSB_CK(cudaMemcpyAsync(h->desc.data(), h->d_desc(), h->desc.size() * 8, cudaMemcpyDeviceToHost, st));
+    RSB_CK(cudaMemcpyAsync(h->lower.data(), h->d_lower(), h->lower.size() * 8, cudaMemcpyDeviceToHost, st));
+    RSB_CK(cudaMemcpyAsync(h->upper_cum.data(), h->d_cum(), h->upper_cum.size() * 8, cudaMemcpyDeviceToHost, st));
+    RSB_CK(cudaMemcpyAsync(h->upper_pos.data(), h->d_pos(), h->upper_pos.size() * 8, cudaMemcpyDeviceToHost, st));
+    RSB_CK(cudaMemcpyAsync(h->jump.data(), h->d_jump(), h->jump.size() * 8, cudaMemcpyDeviceToHost, st));
+    RSB_CK(cudaStreamSynchronize(st));
+    h->host_valid = true;
+    return RSB_OK;
+}
+
+// The build proper. keys128 is device memory holding n (first, second) pairs.
+rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint64_t bucket_size, uint32_t leaf,
+                        uint32_t flags, rsb_mphf **out, bool keep_seeds) {
+    const bool rotate = (flags & RSB_ROTATE) != 0;
+    const LeafTables &lt = leaf_tables(leaf, rotate);
+    if (!shape_matches_kernels(lt.shape)) return RSB_ERR_INTERNAL;
+    DevTables tab;
+    rsb_status rs = get_device_tables(e, lt, leaf, rotate, tab);
+    if (rs != RSB_OK) return rs;
+    cudaStream_t st = e->stream;
+    const uint64_t nb = std::max<uint64_t>(1, (n + bucket_size - 1) / bucket_size);
+    const uint64_t max_nodes = n + 1;
+    const uint32_t nslots = search_slots_needed(e->num_sms);
+
+#define RSB_ENSURE(buf, cnt)                    \
+    do {                                        \
+        rsb_status s_ = ensure(buf, cnt);       \
+        if (s_ != RSB_OK) return s_;            \
+    } while (0)
+    RSB_ENSURE(e->sorted, n);
+    RSB_ENSURE(e->counts, nb);
+    RSB_ENSURE(e->acc, nb + 1);
+    RSB_ENSURE(e->node_count, nb);
+    RSB_ENSURE(e->node_base, nb + 1);
+    RSB_ENSURE(e->scan_tmp, scan_blocks(nb + 1) + 8);
+    RSB_ENSURE(e->nstart, max_nodes);
+    RSB_ENSURE(e->nsize, max_nodes);
+    RSB_ENSURE(e->nstage, max_nodes);
+    RSB_ENSURE(e->seed, max_nodes);
+    RSB_ENSURE(e->nwin, max_nodes);
+    RSB_ENSURE(e->lists, max_nodes);
+    RSB_ENSURE(e->stage_info, 3 * kNumStages);
+    RSB_ENSURE(e->sched, kNumStages);
+    RSB_ENSURE(e->slots, nslots);
+    RSB_ENSURE(e->bits, nb);
+    RSB_ENSURE(e->fixed_bits, nb);
+    RSB_ENSURE(e->pos_acc, nb + 1);
+    RSB_ENSURE(e->status, 1);
+    RSB_ENSURE(e->efp, 1);
+
+    auto *h = new (std::nothrow) rsb_mphf;
+    if (!h) return RSB_ERR_OOM;
+    h->leaf = leaf;
+    h->rotate = rotate;
+    h->bucket_size = bucket_size;
+    h->keys_count = n;
+    h->nbuckets = nb;
+    h->tab = &lt;
+    h->device = e->device;
+    // Output capacities (upper bounds; the encoder reports the exact sizes).
+    h->desc_cap = (8 * n + 65536) / 64 + 16;
+    h->lower_cap = ((nb + 1) * 56 + 63) / 64 + 2;
+    h->cum_cap = (3 * (nb + 1) + 63) / 64 + 2;
+    h->pos_cap = h->cum_cap;
+    h->jump_cap = jump_words_for(nb) + 2;
+    const uint64_t block_words = h->desc_cap + h->lower_cap + h->cum_cap + h->pos_cap + h->jump_cap;
+    if (cudaMallocAsync((void **)&h->d_block, block_words * 8, st) != cudaSuccess) {
+        cudaGetLastError();
+        delete h;
+        return RSB_ERR_OOM;
+    }
+    auto fail = [&](rsb_status s) {
+        if (h->d_block) cudaFreeAsync(h->d_block, st);
+        cudaStreamSynchronize(st);
+        delete h;
+        return s;
+    };
+#define RSB_CKH(call)                         \
+    do {                                      \
+        cudaError_t e_ = (call);              \
+        if (e_ != cudaSuccess) {              \
+            g_last_cuda = e_;                 \
+            return fail(RSB_ERR_CUDA);        \
+        }                                     \
+    } while (0)
+
+    NodeArrays nodes{e->nstart.p, e->nsize.p, e->nstage.p, e->seed.p, e->nwin.p};
+    ScanTmp stmp{e->scan_tmp.p, e->scan_tmp.cap};
+    const uint64_t *node_total = e->node_base.p + nb;
+
+    RSB_CKH(cudaEventRecord(e->ev[0], st));
+    RSB_CKH(cudaMemsetAsync(e->status.p, 0, sizeof(DevStatus), st));
+    RSB_CKH(cudaMemsetAsync(e->efp.p, 0, sizeof(EfParams), st));
+    RSB_CKH(cudaMemsetAsync(e->sched.p, 0, kNumStages * sizeof(uint32_t), st));
+
+    // ---- buckets ----
+    launch_bucket_count(keys128, n, nb, e->counts.p, st);
+    launch_bucket_check(e->counts.p, nb, e->status.p, st);
+    exclusive_scan_u32(e->counts.p, e->acc.p, nb, stmp, st);
+    launch_bucket_scatter(keys128, n, nb, e->acc.p, e->counts.p, e->sorted.p, st);
+    launch_bucket_sort(e->sorted.p, e->acc.p, nb, e->status.p, st);
+    // ---- tree ----
+    launch_bucket_nodes(e->acc.p, nb, tab, e->node_count.p, st);
+    exclusive_scan_u32(e->node_count.p, e->node_base.p, nb, stmp, st);
+    RSB_CKH(cudaMemsetAsync(e->seed.p, 0xFF, max_nodes * sizeof(uint64_t), st));
+    RSB_CKH(cudaMemsetAsync(e->nwin.p, 0, max_nodes * sizeof(uint32_t), st));
+    launch_tree_emit(e->acc.p, nb, e->node_base.p, lt.shape, nodes, st);
+    launch_stage_lists(e->nstage.p, node_total, (uint32_t)max_nodes, e->stage_info.p, e->lists.p, st);
+    RSB_CKH(cudaGetLastError());
+    RSB_CKH(cudaEventRecord(e->ev[1], st));
+
+    // ---- searches ----
+    SearchCtx sc{};
+    sc.sh = lt.shape;
+    sc.node_total = node_total;
+    sc.stage_info = e->stage_info.p;
+    sc.lists = e->lists.p;
+    sc.nodes = nodes;
+    sc.keys = e->sorted.p;
+    sc.tab = tab;
+    sc.status = e->status.p;
+    sc.sched = e->sched.p;
+    sc.slots = e->slots.p;
+    sc.nslots = nslots;
+    sc.budget_shift = e->budget_shift;
+    sc.budget_min = e->budget_min;
+    sc.num_sms = e->num_sms;
+    for (uint32_t d = 0; d < lt.max_higher_depth && d < (uint32_t)kMaxHigherDepth; ++d) {
+        search_higher(sc, (int)d, st);
+        RSB_CKH(cudaEventRecord(e->ev[2 + d], st));
+    }
+    for (int stage : {kStageUpper, kStageLower}) {
+        RSB_CKH(cudaMemsetAsync(e->slots.p, 0xFF, nslots * sizeof(uint32_t), st));
+        search_aggr(sc, stage, st);
+        partition_aggr(sc, stage, st);
+        RSB_CKH(cudaEventRecord(e->ev[2 + stage], st));
+    }
+    for (int stage : {kStageLeafRot, kStageLeafBF}) {
+        RSB_CKH(cudaMemsetAsync(e->slots.p, 0xFF, nslots * sizeof(uint32_t), st));
+        search_leaves(sc, stage, st);
+        RSB_CKH(cudaEventRecord(e->ev[2 + stage], st));
+    }
+    RSB_CKH(cudaGetLastError());
+
+    // ---- encoding ----
+    launch_bucket_bits(e->node_base.p, nb, nodes, tab, e->bits.p, e->fixed_bits.p, e->status.p, st);
+    exclusive_scan_u32(e->bits.p, e->pos_acc.p, nb, stmp, st);
+    RSB_CKH(cudaMemsetAsync(h->d_block, 0, block_words * 8, st));
+    launch_write_rice(e->node_base.p, nb, nodes, tab, e->pos_acc.p, e->fixed_bits.p, h->d_desc(), h->desc_cap, e->efp.p,
+                      e->status.p, st);
+    launch_ef_build(e->acc.p, e->pos_acc.p, nb, n, e->efp.p, h->d_lower(), h->lower_cap, h->d_cum(), h->cum_cap,
+                    h->d_pos(), h->pos_cap, h->d_jump(), h->jump_cap, e->status.p, st);
+    launch_evals(node_total, nodes, leaf, rotate ? 1 : 0, e->efp.p, st);
+    RSB_CKH(cudaGetLastError());
+    RSB_CKH(cudaEventRecord(e->ev[kNumEvents - 1], st));
+
+    DevStatus dst{};
+    uint32_t stage_counts[kNumStages];
+    RSB_CKH(cudaMemcpyAsync(&dst, e->status.p, sizeof(dst), cudaMemcpyDeviceToHost, st));
+    RSB_CKH(cudaMemcpyAsync(&h->ef, e->efp.p, sizeof(EfParams), cudaMemcpyDeviceToHost, st));
+    RSB_CKH(cudaMemcpyAsync(stage_counts, e->stage_info.p, sizeof(stage_counts), cudaMemcpyDeviceToHost, st));
+    RSB_CKH(cudaStreamSynchronize(st));
+    if (dst.code != 0) return fail((rsb_status)dst.code);
+
+    // stats
+    rsb_stats &S = h->stats;
+    S.keys = n;
+    S.buckets = nb;
+    S.evals_alg = h->ef.evals_alg;
+    S.descriptor_bits = h->ef.total_bits;
+    uint64_t tot = 0;
+    for (int s = 0; s < kNumStages; ++s) {
+        S.nodes_per_stage[s] = stage_counts[s];
+        tot += stage_counts[s];
+    }
+    S.nodes = tot;
+    S.ms_total = elapsed(e->ev[0], e->ev[kNumEvents - 1]);
+    S.ms_partition = elapsed(e->ev[0], e->ev[1]);
+    cudaEvent_t prev = e->ev[1];
+    for (int s = 0; s < kNumStages; ++s) {
+        const bool recorded = (s < (int)lt.max_higher_depth && s < kMaxHigherDepth) || s >= kStageUpper;
+        if (!recorded) continue;
+        S.ms_search[s] = elapsed(prev, e->ev[2 + s]);
+        prev = e->ev[2 + s];
+    }
+    S.ms_encode = elapsed(prev, e->ev[kNumEvents - 1]);
+
+    if (keep_seeds) {
+        h->seeds.resize(tot);
+        h->sizes.resize(tot);
+        std::vector<uint16_t> sz(tot);
+        if (tot) {
+            RSB_CKH(cudaMemcpy(h->seeds.data(), e->seed.p, tot * 8, cudaMemcpyDeviceToHost));
+            RSB_CKH(cudaMemcpy(sz.data(), e->nsize.p, tot * 2, cudaMemcpyDeviceToHost));
+        }
+        for (uint64_t i = 0; i < tot; ++i) h->sizes[i] = sz[i];
+    }
+    if (!(flags & RSB_DEVICE_ONLY)) {
+        rsb_status s = copy_to_host(h, st);
+        if (s != RSB_OK) return fail(s);
+    }
+    *out = h;
+    return RSB_OK;
+}
+
+rsb_status check_common(rsb_engine *e, uint64_t n, uint64_t bucket_size, uint32_t leaf, rsb_mphf **out) {
+    if (!e || !out) return RSB_ERR_BAD_ARG;
+    if (leaf < 2 || leaf > (uint32_t)kMaxLeafSize || bucket_size == 0) return RSB_ERR_BAD_ARG;
+    if (n >= (1ull << 32) - 1) return RSB_ERR_BAD_ARG;
+    if (cudaSetDevice(e->device) != cudaSuccess) {
+        cudaGetLastError();
+        return RSB_ERR_CUDA;
+    }
+    return RSB_OK;
+}
+
+constexpr uint32_t kKeepSeeds = RSB_KEEP_SEEDS;
+
+}  // namespace
+
+extern "C" {
+
+const char *rsb_version(void) { return "rsb 0.1 (sm_100a)"; }
+
+rsb_status rsb_golomb_memo(uint32_t leaf, uint32_t *out) {
+    if (leaf < 2 || leaf > (uint32_t)kMaxLeafSize || !out) return RSB_ERR_BAD_ARG;
+    const LeafTables &t = leaf_tables(leaf, true);
+    std::memcpy(out, t.memo.data(), kMaxBucketSize * sizeof(uint32_t));
+    return RSB_OK;
+}
+
+const char *rsb_strerror(rsb_status s) {
+    switch (s) {
+        case RSB_OK: return "ok";
+        case RSB_ERR_BAD_ARG: return "invalid argument";
+        case RSB_ERR_CUDA: return cudaGetErrorString(g_last_cuda);
+        case RSB_ERR_OOM: return "out of memory";
+        case RSB_ERR_DUPLICATE_KEY: return "duplicate key (two keys share a bucket and their second hash half)";
+        case RSB_ERR_SEARCH_BUDGET: return "seed search exceeded its candidate budget";
+        case RSB_ERR_BUCKET_TOO_LARGE: return "bucket with 3000 or more keys";
+        case RSB_ERR_TIMEOUT: return "bounded device wait timed out";
+        case RSB_ERR_FORMAT: return "malformed serialized function or leaf size mismatch";
+        case RSB_ERR_INTERNAL: return "internal error";
+        case RSB_ERR_NO_DEVICE: return "no usable CUDA device";
+    }
+    return "unknown status";
+}
+
+rsb_status rsb_engine_create(int device, void *stream, rsb_engine **out) {
+    if (!out) return RSB_ERR_BAD_ARG;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+        cudaGetLastError();
+        return RSB_ERR_NO_DEVICE;
+    }
+    RSB_CK(cudaSetDevice(device));
+    cudaDeviceProp prop{};
+    RSB_CK(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) return RSB_ERR_NO_DEVICE;  // kernels are built for sm_100a only
+    auto *e = new (std::nothrow) rsb_engine;
+    if (!e) return RSB_ERR_OOM;
+    e->device = device;
+    e->num_sms = prop.multiProcessorCount;
+    if (stream) {
+        e->stream = (cudaStream_t)stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete e;
+            return RSB_ERR_CUDA;
+        }
+        e->own_stream = true;
+    }
+    for (auto &ev : e->ev) cudaEventCreate(&ev);
+    // Keep freed pool memory cached: handles are allocated stream-ordered on every build.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t thr = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    cudaGetLastError();
+    *out = e;
+    return RSB_OK;
+}
+
+rsb_status rsb_engine_destroy(rsb_engine *e) {
+    if (!e) return RSB_ERR_BAD_ARG;
+    cudaSetDevice(e->device);
+    cudaStreamSynchronize(e->stream);
+    release(e->keys128); release(e->raw_u64); release(e->offsets); release(e->sorted); release(e->acc);
+    release(e->node_base); release(e->scan_tmp); release(e->pos_acc); release(e->seed); release(e->counts);
+    release(e->node_count); release(e->lists); release(e->stage_info); release(e->sched); release(e->slots);
+    release(e->bits); release(e->fixed_bits); release(e->nstart); release(e->nwin); release(e->nsize);
+    release(e->nstage); release(e->bytes); release(e->status); release(e->efp);
+    for (auto &kv : e->tables) cudaFree(kv.second.first);
+    for (auto &ev : e->ev) cudaEventDestroy(ev);
+    if (e->own_stream) cudaStreamDestroy(e->stream);
+    delete e;
+    return RSB_OK;
+}
+
+rsb_status rsb_engine_set_budget(rsb_engine *e, uint32_t shift, uint64_t min_candidates) {
+    if (!e || shift > 62) return RSB_ERR_BAD_ARG;
+    e->budget_shift = shift;
+    e->budget_min = min_candidates;
+    return RSB_OK;
+}
+
+static rsb_status stage_keys128(rsb_engine *e, const rsb_hash128 *keys, uint64_t n, uint32_t flags, const uint64_t **dk) {
+    if (flags & RSB_KEYS_ON_DEVICE) {
+        *dk = (const uint64_t *)keys;
+        return RSB_OK;
+    }
+    rsb_status s = ensure(e->keys128, 2 * n);
+    if (s != RSB_OK) return s;
+    if (n) RSB_CK(cudaMemcpyAsync(e->keys128.p, keys, n * 16, cudaMemcpyHostToDevice, e->stream));
+    *dk = e->keys128.p;
+    return RSB_OK;
+}
+
+rsb_status rsb_build_hash128(rsb_engine *e, const rsb_hash128 *keys, uint64_t n, uint64_t bucket_size, uint32_t leaf,
+                             uint32_t flags, rsb_mphf **out) {
+    rsb_status s = check_common(e, n, bucket_size, leaf, out);
+    if (s != RSB_OK) return s;
+    if (n && !keys) return RSB_ERR_BAD_ARG;
+    const uint64_t *dk = nullptr;
+    s = stage_keys128(e, keys, n, flags, &dk);
+    if (s != RSB_OK) return s;
+    return build_device(e, dk, n, bucket_size, leaf, flags, out, (flags & kKeepSeeds) != 0);
+}
+
+rsb_status rsb_build_u64(rsb_engine *e, const uint64_t *keys, uint64_t n, uint64_t bucket_size, uint32_t leaf,
+                         uint32_t flags, rsb_mphf **out) {
+    rsb_status s = check_common(e, n, bucket_size, leaf, out);
+    if (s != RSB_OK) return s;
+    if (n && !keys) return RSB_ERR_BAD_ARG;
+    const uint64_t *dk = keys;
+    if (!(flags & RSB_KEYS_ON_DEVICE)) {
+        s = ensure(e->raw_u64, n);
+        if (s != RSB_OK) return s;
+        if (n) RSB_CK(cudaMemcpyAsync(e->raw_u64.p, keys, n * 8, cudaMemcpyHostToDevice, e->stream));
+        dk = e->raw_u64.p;
+    }
+    s = ensure(e->keys128, 2 * n);
+    if (s != RSB_OK) return s;
+    launch_hash_u64(dk, n, e->keys128.p, e->stream);
+    return build_device(e, e->keys128.p, n, bucket_size, leaf, flags, out, (flags & kKeepSeeds) != 0);
+}
+
+static rsb_status stage_strings(rsb_engine *e, const uint8_t *bytes, const uint64_t *offsets, uint64_t n, uint32_t flags,
+                                const uint8_t **db, const uint64_t **doff) {
+    if (flags & RSB_KEYS_ON_DEVICE) {
+        *db = bytes;
+        *doff = offsets;
+        return RSB_OK;
+    }
+    const uint64_t nbytes = offsets[n];
+    rsb_status s = ensure(e->bytes, nbytes);
+    if (s != RSB_OK) return s;
+    s = ensure(e->offsets, n + 1);
+    if (s != RSB_OK) return s;
+    if (nbytes) RSB_CK(cudaMemcpyAsync(e->bytes.p, bytes, nbytes, cudaMemcpyHostToDevice, e->stream));
+    RSB_CK(cudaMemcpyAsync(e->offsets.p, offsets, (n + 1) * 8, cudaMemcpyHostToDevice, e->stream));
+    *db = e->bytes.p;
+    *doff = e->offsets.p;
+    return RSB_OK;
+}
+
+rsb_status rsb_build_strings(rsb_engine *e, const uint8_t *bytes, const uint64_t *offsets, uint64_t n,
+                             uint64_t bucket_size, uint32_t leaf, uint32_t flags, rsb_mphf **out) {
+    rsb_status s = check_common(e, n, bucket_size, leaf, out);
+    if (s != RSB_OK) return s;
+    if (!offsets) return RSB_ERR_BAD_ARG;
+    const uint8_t *db;
+    const uint64_t *doff;
+    s = stage_strings(e, bytes, offsets, n, flags, &db, &doff);
+    if (s != RSB_OK) return s;
+    s = ensure(e->keys128, 2 * n);
+    if (s != RSB_OK) return s;
+    launch_hash_strings(db, doff, n, e->keys128.p, e->stream);
+    return build_device(e, e->keys128.p, n, bucket_size, leaf, flags, out, (flags & kKeepSeeds) != 0);
+}
+
+rsb_status rsb_hash_strings(rsb_engine *e, const uint8_t *bytes, const uint64_t *offsets, uint64_t n, uint32_t flags,
+                            rsb_hash128 *out) {
+    if (!e || !offsets || !out) return RSB_ERR_BAD_ARG;
+    RSB_CK(cudaSetDevice(e->device));
+    const uint8_t *db;
+    const uint64_t *doff;
+    rsb_status s = stage_strings(e, bytes, offsets, n, flags, &db, &doff);
+    if (s != RSB_OK) return s;
+    s = ensure(e->keys128, 2 * n);
+    if (s != RSB_OK) return s;
+    launch_hash_strings(db, doff, n, e->keys128.p, e->stream);
+    RSB_CK(cudaGetLastError());
+    RSB_CK(cudaMemcpyAsync(out, e->keys128.p, n * 16, (flags & RSB_KEYS_ON_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                           e->stream));
+    RSB_CK(cudaStreamSynchronize(e->stream));
+    return RSB_OK;
+}
+
+rsb_status rsb_hash_u64(rsb_engine *e, const uint64_t *keys, uint64_t n, uint32_t flags, rsb_hash128 *out) {
+    if (!e || (n && (!keys || !out))) return RSB_ERR_BAD_ARG;
+    RSB_CK(cudaSetDevice(e->device));
+    const uint64_t *dk = keys;
+    if (!(flags & RSB_KEYS_ON_DEVICE)) {
+        rsb_status s = ensure(e->raw_u64, n);
+        if (s != RSB_OK) return s;
+        if (n) RSB_CK(cudaMemcpyAsync(e->raw_u64.p, keys, n * 8, cudaMemcpyHostToDevice, e->stream));
+        dk = e->raw_u64.p;
+    }
+    rsb_status s = ensure(e->keys128, 2 * n);
+    if (s != RSB_OK) return s;
+    launch_hash_u64(dk, n, e->keys128.p, e->stream);
+    RSB_CK(cudaGetLastError());
+    if (n)
+        RSB_CK(cudaMemcpyAsync(out, e->keys128.p, n * 16, (flags & RSB_KEYS_ON_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                               e->stream));
+    RSB_CK(cudaStreamSynchronize(e->stream));
+    return RSB_OK;
+}
+
+static rsb_status ensure_host(rsb_mphf *h) {
+    if (h->host_valid) return RSB_OK;
+    cudaStream_t st = nullptr;
+    if (h->device >= 0) cudaSetDevice(h->device);
+    return copy_to_host(h, st);
+}
+
+rsb_status rsb_query_hash128(rsb_mphf *h, const rsb_hash128 *keys, uint64_t n, uint64_t *out) {
+    if (!h || (n && (!keys || !out))) return RSB_ERR_BAD_ARG;
+    rsb_status s = ensure_host(h);
+    if (s != RSB_OK) return s;
+    const MphfView v = h->host_view();
+    for (uint64_t i = 0; i < n; ++i) out[i] = mphf_query(v, keys[i].first, keys[i].second);
+    return RSB_OK;
+}
+
+rsb_status rsb_query_strings(rsb_mphf *h, const uint8_t *bytes, const uint64_t *offsets, uint64_t n, uint64_t *out) {
+    if (!h || !offsets || (n && !out)) return RSB_ERR_BAD_ARG;
+    rsb_status s = ensure_host(h);
+    if (s != RSB_OK) return s;
+    const MphfView v = h->host_view();
+    for (uint64_t i = 0; i < n; ++i) {
+        uint64_t h0 = 0, h1 = 0;
+        spooky128(bytes + offsets[i], offsets[i + 1] - offsets[i], h0, h1);
+        out[i] = mphf_query(v, h1, h0);
+    }
+    return RSB_OK;
+}
+
+rsb_status rsb_query_device(rsb_engine *e, rsb_mphf *h, const rsb_hash128 *keys, uint64_t n, uint64_t *out) {
+    if (!e || !h || (n && (!keys || !out))) return RSB_ERR_BAD_ARG;
+    RSB_CK(cudaSetDevice(e->device));
+    if (!h->d_block || h->device != e->device) {
+        // upload a host-side (e.g. deserialized) function
+        rsb_status s = ensure_host(h);
+        if (s != RSB_OK) return s;
+        if (h->d_block) cudaFree(h->d_block);
+        h->desc_cap = h->desc.size();
+        h->lower_cap = h->lower.size();
+        h->cum_cap = h->upper_cum.size();
+        h->pos_cap = h->upper_pos.size();
+        h->jump_cap = h->jump.size();
+        const uint64_t words = h->desc_cap + h->lower_cap + h->cum_cap + h->pos_cap + h->jump_cap + 1;
+        RSB_CK(cudaMalloc((void **)&h->d_block, words * 8));
+        RSB_CK(cudaMemcpy(h->d_desc(), h->desc.data(), h->desc.size() * 8, cudaMemcpyHostToDevice));
+        RSB_CK(cudaMemcpy(h->d_lower(), h->lower.data(), h->lower.size() * 8, cudaMemcpyHostToDevice));
+        RSB_CK(cudaMemcpy(h->d_cum(), h->upper_cum.data(), h->upper_cum.size() * 8, cudaMemcpyHostToDevice));
+        RSB_CK(cudaMemcpy(h->d_pos(), h->upper_pos.data(), h->upper_pos.size() * 8, cudaMemcpyHostToDevice));
+        RSB_CK(cudaMemcpy(h->d_jump(), h->jump.data(), h->jump.size() * 8, cudaMemcpyHostToDevice));
+        h->device = e->device;
+    }
+    DevTables tab;
+    rsb_status s = get_device_tables(e, *h->tab, h->leaf, h->rotate, tab);
+    if (s != RSB_OK) return s;
+    MphfView v{};
+    v.sh = h->tab->shape;
+    v.nbuckets = h->nbuckets;
+    v.desc = h->d_desc();
+    v.desc_words = h->ef.desc_words;
+    v.u_cum_keys = h->ef.u_cum_keys;
+    v.u_position = h->ef.u_position;
+    v.l_cum_keys = h->ef.l_cum_keys;
+    v.l_position = h->ef.l_position;
+    v.cum_keys_min_delta = h->ef.cum_keys_min_delta;
+    v.min_diff = h->ef.min_diff;
+    v.bits_per_key_fixed_point = h->ef.bits_per_key_fixed_point;
+    v.lower = h->d_lower();
+    v.upper_cum = h->d_cum();
+    v.upper_pos = h->d_pos();
+    v.jump = h->d_jump();
+    v.lower_words = h->ef.lower_words;
+    v.cum_words = h->ef.cum_words;
+    v.pos_words = h->ef.pos_words;
+    v.jump_words = h->ef.jump_words;
+    v.memo = tab.memo;
+    launch_query_view(v, (const uint64_t *)keys, n, out, e->stream);
+    RSB_CK(cudaGetLastError());
+    RSB_CK(cudaStreamSynchronize(e->stream));
+    return RSB_OK;
+}
+
+// bitCountCumKeys + bitCountPosition (DoubleEF.hpp:435-437) + descriptors.getBits()
+// (RiceBitVector.hpp:152); the C++ wrapper adds 8 * sizeof(*this) like getBits() does.
+rsb_status rsb_get_bits(rsb_mphf *h, uint64_t *bits) {
+    if (!h || !bits) return RSB_ERR_BAD_ARG;
+    const EfParams &f = h->ef;
+    const uint64_t nb = f.num_buckets;
+    const uint64_t jh = f.jump_words / 2;
+    const uint64_t cum = (nb + 1) * f.l_cum_keys + nb + 1 + (f.u_cum_keys >> f.l_cum_keys) + jh;
+    const uint64_t pos = (nb + 1) * f.l_position + nb + 1 + (f.u_position >> f.l_position) + jh;
+    *bits = cum + pos + f.desc_words * 64;
+    return RSB_OK;
+}
+
+static void put64(std::vector<uint8_t> &o, uint64_t v) {
+    uint8_t b[8];
+    std::memcpy(b, &v, 8);
+    o.insert(o.end(), b, b + 8);
+}
+static void put_vec(std::vector<uint8_t> &o, const std::vector<uint64_t> &v) {
+    put64(o, v.size());
+    const uint8_t *p = (const uint8_t *)v.data();
+    o.insert(o.end(), p, p + v.size() * 8);
+}
+
+// Layout of operator<< (GPURecSplit.cuh:817-825, DoubleEF.hpp:100-113); a word vector is
+// written as a uint64 element count followed by its words.
+rsb_status rsb_serialize(rsb_mphf *h, uint8_t *buf, size_t *len) {
+    if (!h || !len) return RSB_ERR_BAD_ARG;
+    rsb_status s = ensure_host(h);
+    if (s != RSB_OK) return s;
+    const size_t need = 8 * (3 + 1 + h->desc.size() + 6 + 4 + h->lower.size() + h->upper_cum.size() + h->upper_pos.size() +
+                             h->jump.size());
+    if (!buf) {
+        *len = need;
+        return RSB_OK;
+    }
+    if (*len < need) {
+        *len = need;
+        return RSB_ERR_BAD_ARG;
+    }
+    std::vector<uint8_t> o;
+    o.reserve(need);
+    put64(o, h->leaf);
+    put64(o, h->bucket_size);
+    put64(o, h->keys_count);
+    put_vec(o, h->desc);
+    put64(o, h->ef.num_buckets);
+    put64(o, h->ef.u_cum_keys);
+    put64(o, h->ef.u_position);
+    put64(o, (uint64_t)h->ef.cum_keys_min_delta);
+    put64(o, (uint64_t)h->ef.min_diff);
+    put64(o, h->ef.bits_per_key_fixed_point);
+    put_vec(o, h->lower);
+    put_vec(o, h->upper_cum);
+    put_vec(o, h->upper_pos);
+    put_vec(o, h->jump);
+    std::memcpy(buf, o.data(), o.size());
+    *len = o.size();
+    return RSB_OK;
+}
+
+rsb_status rsb_deserialize(const uint8_t *buf, size_t len, uint32_t leaf, uint32_t flags, rsb_mphf **out) {
+    if (!buf || !out) return RSB_ERR_BAD_ARG;
+    size_t off = 0;
+    bool ok = true;
+    auto get64 = [&]() -> uint64_t {
+        if (len - off < 8 || off > len) {
+            ok = false;
+            return 0;
+        }
+        uint64_t v;
+        std::memcpy(&v, buf + off, 8);
+        off += 8;
+        return v;
+    };
+    auto get_vec = [&](std::vector<uint64_t> &v) {
+        const uint64_t n = get64();
+        if (!ok || (len - off) / 8 < n) {
+            ok = false;
+            return;
+        }
+        v.resize(n);
+        std::memcpy(v.data(), buf + off, n * 8);
+        off += n * 8;
+    };
+    const uint64_t l = get64();
+    if (!ok || l != leaf || leaf < 2 || leaf > (uint32_t)kMaxLeafSize) return RSB_ERR_FORMAT;
+    auto *h = new (std::nothrow) rsb_mphf;
+    if (!h) return RSB_ERR_OOM;
+    h->leaf = leaf;
+    h->rotate = (flags & RSB_ROTATE) != 0;
+    h->bucket_size = get64();
+    h->keys_count = get64();
+    if (!ok || h->bucket_size == 0) {
+        delete h;
+        return RSB_ERR_FORMAT;
+    }
+    h->nbuckets = std::max<uint64_t>(1, (h->keys_count + h->bucket_size - 1) / h->bucket_size);  // :499
+    get_vec(h->desc);
+    EfParams &f = h->ef;
+    f.num_buckets = get64();
+    f.u_cum_keys = get64();
+    f.u_position = get64();
+    f.cum_keys_min_delta = (int64_t)get64();
+    f.min_diff = (int64_t)get64();
+    f.bits_per_key_fixed_point = get64();
+    get_vec(h->lower);
+    get_vec(h->upper_cum);
+    get_vec(h->upper_pos);
+    get_vec(h->jump);
+    if (!ok) {
+        delete h;
+        return RSB_ERR_FORMAT;
+    }
+    const uint64_t nb = f.num_buckets;
+    f.l_position = f.u_position / (nb + 1) == 0 ? 0 : 63 - __builtin_clzll(f.u_position / (nb + 1));  // DoubleEF.hpp:123
+    f.l_cum_keys = f.u_cum_keys / (nb + 1) == 0 ? 0 : 63 - __builtin_clzll(f.u_cum_keys / (nb + 1));
+    f.desc_words = h->desc.size();
+    f.lower_words = h->lower.size();
+    f.cum_words = h->upper_cum.size();
+    f.pos_words = h->upper_pos.size();
+    f.jump_words = h->jump.size();
+    h->tab = &leaf_tables(leaf, h->rotate);
+    h->host_valid = true;
+    *out = h;
+    return RSB_OK;
+}
+
+rsb_status rsb_seeds(rsb_mphf *h, uint64_t *seeds, uint32_t *sizes, size_t *count) {
+    if (!h || !count) return RSB_ERR_BAD_ARG;
+    if (!seeds) {
+        *count = h->seeds.size();
+        return RSB_OK;
+    }
+    const size_t n = std::min(*count, h->seeds.size());
+    std::memcpy(seeds, h->seeds.data(), n * 8);
+    if (sizes) std::memcpy(sizes, h->sizes.data(), n * 4);
+    *count = n;
+    return RSB_OK;
+}
+
+rsb_status rsb_get_stats(rsb_mphf *h, rsb_stats *s) {
+    if (!h || !s) return RSB_ERR_BAD_ARG;
+    *s = h->stats;
+    return RSB_OK;
+}
+
+rsb_status rsb_free(rsb_mphf *h) {
+    if (!h) return RSB_ERR_BAD_ARG;
+    if (h->d_block) {
+        cudaSetDevice(h->device);
+        cudaFree(h->d_block);
+    }
+    delete h;
+    return RSB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,92 @@
+// Launchers of the engine's kernels (implemented in rsb_prep.cu, rsb_search.cu, rsb_encode.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "rsb_common.cuh"
+
+namespace rsb {
+
+// Device-side per-leaf constants (uploaded once per engine and leaf size).
+struct DevTables {
+    const uint32_t *memo;   // kMaxBucketSize
+    const uint32_t *nodes;  // kMaxBucketSize
+};
+
+// Scratch of a plain exclusive scan.
+struct ScanTmp {
+    uint64_t *block_sums;
+    size_t blocks_cap;
+};
+
+size_t scan_blocks(size_t n);
+// out[i] = sum_{j<i} in[i] for i <= n (out has n+1 entries); in is u32.
+void exclusive_scan_u32(const uint32_t *in, uint64_t *out, size_t n, ScanTmp tmp, cudaStream_t st);
+
+// ---- preparation (rsb_prep.cu) ----
+void launch_hash_u64(const uint64_t *keys, uint64_t n, uint64_t *out128, cudaStream_t st);
+void launch_hash_strings(const uint8_t *bytes, const uint64_t *offsets, uint64_t n, uint64_t *out128, cudaStream_t st);
+void launch_bucket_count(const uint64_t *keys128, uint64_t n, uint64_t nbuckets, uint32_t *counts, cudaStream_t st);
+void launch_bucket_check(const uint32_t *counts, uint64_t nbuckets, DevStatus *status, cudaStream_t st);
+void launch_bucket_scatter(const uint64_t *keys128, uint64_t n, uint64_t nbuckets, const uint64_t *acc,
+                           uint32_t *cursor, uint64_t *sorted, cudaStream_t st);
+void launch_bucket_sort(uint64_t *sorted, const uint64_t *acc, uint64_t nbuckets, DevStatus *status, cudaStream_t st);
+void launch_bucket_nodes(const uint64_t *acc, uint64_t nbuckets, DevTables tab, uint32_t *node_count, cudaStream_t st);
+void launch_tree_emit(const uint64_t *acc, uint64_t nbuckets, const uint64_t *node_base, Shape sh, NodeArrays nodes,
+                      cudaStream_t st);
+// Stage lists: counting sort of node ids by stage. stage_info holds [kNumStages] counts
+// followed by [kNumStages] bases; lists receives the node ids.
+void launch_stage_lists(const uint8_t *stage, const uint64_t *total_nodes, uint32_t max_nodes, uint32_t *stage_info,
+                        uint32_t *lists, cudaStream_t st);
+
+// ---- search (rsb_search.cu) ----
+struct SearchCtx {
+    Shape sh;
+    const uint64_t *node_total;  // device: number of nodes
+    const uint32_t *stage_info;  // device: counts[kNumStages], bases[kNumStages]
+    const uint32_t *lists;
+    NodeArrays nodes;
+    uint64_t *keys;              // bucket-partitioned key seconds
+    DevTables tab;
+    DevStatus *status;
+    uint32_t *sched;             // per-stage scheduler words (fresh-node counter per stage)
+    uint32_t *slots;             // help slots
+    uint32_t nslots;
+    uint32_t budget_shift;
+    uint64_t budget_min;
+    int num_sms;
+};
+void search_higher(const SearchCtx &c, int depth, cudaStream_t st);
+void search_aggr(const SearchCtx &c, int stage, cudaStream_t st);
+void partition_aggr(const SearchCtx &c, int stage, cudaStream_t st);
+void search_leaves(const SearchCtx &c, int stage, cudaStream_t st);
+uint32_t search_slots_needed(int num_sms);
+
+// ---- encoding (rsb_encode.cu) ----
+struct EfParams {
+    uint64_t num_buckets, u_cum_keys, u_position, l_cum_keys, l_position;
+    int64_t cum_keys_min_delta, min_diff;
+    uint64_t bits_per_key_fixed_point;
+    uint64_t lower_words, cum_words, pos_words, jump_words;
+    uint64_t total_bits;       // descriptor bits before the sentinel
+    uint64_t desc_words;       // descriptor words incl. the sentinel
+    uint64_t evals_alg;
+};
+void launch_bucket_bits(const uint64_t *node_base, uint64_t nbuckets, NodeArrays nodes, DevTables tab,
+                        uint32_t *bits, uint32_t *fixed_bits, DevStatus *status, cudaStream_t st);
+void launch_write_rice(const uint64_t *node_base, uint64_t nbuckets, NodeArrays nodes, DevTables tab,
+                       const uint64_t *pos_acc, const uint32_t *fixed_bits, uint64_t *desc, uint64_t desc_cap_words,
+                       EfParams *ef, DevStatus *status, cudaStream_t st);
+void launch_ef_build(const uint64_t *cum, const uint64_t *pos, uint64_t nbuckets, uint64_t keys, EfParams *ef,
+                     uint64_t *lower, uint64_t lower_cap, uint64_t *upper_cum, uint64_t cum_cap, uint64_t *upper_pos,
+                     uint64_t pos_cap, uint64_t *jump, uint64_t jump_cap, DevStatus *status, cudaStream_t st);
+void launch_evals(const uint64_t *node_total, NodeArrays nodes, uint32_t leaf, uint32_t rotate, EfParams *ef,
+                  cudaStream_t st);
+
+// ---- queries (rsb_query.cu) ----
+struct MphfView;
+void launch_query_view(const MphfView &f, const uint64_t *keys128, uint64_t n, uint64_t *out, cudaStream_t st);
+bool shape_matches_kernels(const Shape &s);
+
+}  // namespace rsb

@@ -1,0 +1,549 @@
+// Seed searches of RecSplit construction on sm_100a.
+//
+// Every search returns the minimum seed x >= 0 (counted from the level's start seed) for
+// which the node's keys split as required, as SIMDRecSplit does:
+//   fanout-2 split      SIMDRecSplit.hpp:250-317   (GPURecSplit.cuh:107-156)
+//   aggregation levels  SIMDRecSplit.hpp:319-423   (GPURecSplit.cuh:164-264)
+//   leaf, brute force   SIMDRecSplit.hpp:510-599   (GPURecSplit.cuh:351-392)
+//   leaf, rotation      SIMDRecSplit.hpp:452-509   (GPURecSplit.cuh:309-350)
+//
+// Work distribution. Fanout-2 nodes (few, cheap) get one CTA each, which searches and then
+// partitions the node in place. Aggregation nodes and leaves are searched by persistent
+// warps: a node hands out ascending windows of W candidate seeds from an atomic counter;
+// the warp that took the node from the stage list owns it, and warps that run out of fresh
+// nodes help unfinished ones (taking further windows of the same node). A window whose
+// first seed is not below the node's current best is never evaluated, every other window
+// is evaluated completely, and successes are merged with atomicMin — so at kernel end each
+// node holds the minimum successful seed, independent of scheduling. No warp ever waits on
+// another warp: the kernels contain no spin loops.
+#include <cstdio>
+
+#include "rsb_kernels.cuh"
+
+namespace rsb {
+
+namespace {
+
+constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+constexpr int kWarpsPerCta = 8;
+constexpr int kThreads = kWarpsPerCta * 32;
+
+// (lower_aggr, upper_aggr) per leaf size 2..24, the values of AbstractParallelRecSplit.hpp:133,135;
+// checked against make_shape() when an engine first uses a leaf size.
+__host__ __device__ constexpr uint32_t lower_of(int leaf) {
+    constexpr uint32_t t[25] = {0, 0, 4, 6, 8, 15, 18, 21, 32, 36, 40, 55, 60, 78, 84, 90, 112, 119, 126, 152, 160, 168, 198, 207, 216};
+    return t[leaf];
+}
+__host__ __device__ constexpr uint32_t upper_of(int leaf) {
+    constexpr uint32_t t[25] = {0, 0, 8, 12, 16, 30, 36, 63, 96, 108, 120, 220, 240, 312, 336, 450, 560, 595, 630, 760, 960, 1008, 1188, 1242, 1296};
+    return t[leaf];
+}
+
+__device__ __forceinline__ uint64_t vload64(const uint64_t *p) { return *(const volatile uint64_t *)p; }
+__device__ __forceinline__ uint32_t vload32(const uint32_t *p) { return *(const volatile uint32_t *)p; }
+__device__ __forceinline__ int status_code(const DevStatus *s) { return *(const volatile int *)&s->code; }
+
+// shl.b32 clamps shift amounts >= 32 to 32 (result 0), PTX ISA "shl".
+__device__ __forceinline__ uint32_t shl_clamp(uint32_t a, uint32_t b) {
+    uint32_t d;
+    asm("shl.b32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
+
+// Low 16 bits of remix32(hi ^ lo) of a 64-bit candidate.
+__device__ __forceinline__ uint32_t hash16(uint64_t v) { return remix32(uint32_t(v >> 32) ^ uint32_t(v)) & 0xFFFFu; }
+
+__device__ __forceinline__ uint64_t budget_for(const SearchCtx &c, uint32_t m) {
+    const uint32_t g = c.tab.memo[m] >> 27;
+    const uint32_t sh = min(g + c.budget_shift, 62u);
+    const uint64_t b = 1ull << sh;
+    return b > c.budget_min ? b : c.budget_min;
+}
+
+// Scans the help slots (node ids of owners, from a pseudo-random start) for a node of the
+// current stage whose search has not found a seed yet.
+__device__ uint32_t find_help(const SearchCtx &c, uint32_t start) {
+    const int lane = threadIdx.x & 31;
+    for (uint32_t k = 0; k < c.nslots; k += 32) {
+        uint32_t idx = start + k + lane;
+        while (idx >= c.nslots) idx -= c.nslots;
+        const uint32_t nd = (k + lane < c.nslots) ? vload32(&c.slots[idx]) : kEmpty;
+        const bool cand = nd != kEmpty && vload64(&c.nodes.seed[nd]) == kSeedNotFound;
+        const unsigned b = __ballot_sync(0xffffffffu, cand);
+        if (b) return __shfl_sync(0xffffffffu, nd, __ffs(b) - 1);
+    }
+    return kEmpty;
+}
+
+// ---------------------------------------------------------------------------------------
+// Fanout-2 nodes: one CTA per node, search and stable 2-way partition.
+// remap(k + x, m) < split  <=>  hash16(k + x) < ceil(split * 2^16 / m).
+// ---------------------------------------------------------------------------------------
+constexpr int kHigherSeedsPerThread = 2;
+
+__global__ void __launch_bounds__(kThreads) k_search_higher(SearchCtx c, int depth) {
+    extern __shared__ uint64_t sk[];
+    __shared__ unsigned long long s_best;
+    __shared__ uint32_t s_warp[kWarpsPerCta];
+    __shared__ int s_stop;
+    const uint32_t count = c.stage_info[depth];
+    const uint32_t base = c.stage_info[kNumStages + depth];
+    const uint64_t seed = start_seed(depth);
+    const uint32_t upper = c.sh.upper;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint32_t li = blockIdx.x; li < count; li += gridDim.x) {
+        if (threadIdx.x == 0) s_stop = status_code(c.status);
+        __syncthreads();
+        if (s_stop) return;
+        const uint32_t id = c.lists[base + li];
+        const uint32_t start = c.nodes.start[id];
+        const uint32_t m = c.nodes.size[id];
+        const uint32_t split = upper * (uint16_t(m / 2 + upper - 1) / upper);
+        const uint32_t thr = (uint32_t)((((uint64_t)split << 16) + m - 1) / m);
+        for (uint32_t i = threadIdx.x; i < m; i += kThreads) sk[i] = c.keys[start + i];
+        if (threadIdx.x == 0) s_best = kSeedNotFound;
+        __syncthreads();
+        const uint64_t budget = budget_for(c, m);
+        constexpr uint32_t W = kThreads * kHigherSeedsPerThread;
+        bool failed = false;
+        for (uint64_t x0 = 0;; x0 += W) {
+#pragma unroll
+            for (int s = 0; s < kHigherSeedsPerThread; ++s) {
+                const uint64_t x = x0 + threadIdx.x + (uint64_t)s * kThreads;
+                const uint64_t sx = seed + x;
+                uint32_t cnt = 0;
+                for (uint32_t i = 0; i < m; ++i) cnt += hash16(sk[i] + sx) < thr;
+                if (cnt == split) atomicMin(&s_best, (unsigned long long)x);
+            }
+            __syncthreads();
+            const bool done = s_best != kSeedNotFound;
+            __syncthreads();
+            if (done) break;
+            if (x0 + W >= budget) {
+                failed = true;
+                break;
+            }
+        }
+        const uint64_t x = failed ? kSeedFailed : (uint64_t)s_best;
+        if (threadIdx.x == 0) c.nodes.seed[id] = x;
+        if (failed) {
+            if (threadIdx.x == 0) set_error(c.status, RSB_ERR_SEARCH_BUDGET, id);
+            return;
+        }
+        // Stable partition: keys remapping below `split` first (SIMDRecSplit.hpp:288-306).
+        const uint32_t per = (m + kThreads - 1) / kThreads;
+        const uint32_t b0 = min(m, threadIdx.x * per), b1 = min(m, b0 + per);
+        const uint64_t sx = seed + x;
+        uint32_t left = 0;
+        for (uint32_t i = b0; i < b1; ++i) left += hash16(sk[i] + sx) < thr;
+        // block exclusive scan of `left`
+        uint32_t inc = left;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t o = __shfl_up_sync(0xffffffffu, inc, d);
+            if (lane >= d) inc += o;
+        }
+        if (lane == 31) s_warp[warp] = inc;
+        __syncthreads();
+        uint32_t wbase = 0;
+        for (int w = 0; w < warp; ++w) wbase += s_warp[w];
+        uint32_t lpos = wbase + inc - left;
+        uint32_t rpos = split + (b0 - lpos);
+        for (uint32_t i = b0; i < b1; ++i) {
+            const uint64_t k = sk[i];
+            if (hash16(k + sx) < thr) c.keys[start + lpos++] = k;
+            else c.keys[start + rpos++] = k;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Aggregation levels. Part counts are packed in bytes: parts 0-3 in `lo`, 4-7 in `hi`; with
+// fanout 9 the last part is implied by the others. Every target is below 255 and a node
+// holds at most fanout * SPLIT keys, so a byte can only carry into the next one on
+// candidates that already fail — packed equality is exact equality.
+// ---------------------------------------------------------------------------------------
+constexpr int kAggrSeedsPerLane = 4;
+
+template <int LEAF, int STAGE>
+struct AggrCfg {
+    static constexpr uint32_t SPLIT = STAGE == kStageUpper ? lower_of(LEAF) : (uint32_t)LEAF;
+    static constexpr uint32_t MAXM = STAGE == kStageUpper ? upper_of(LEAF) : lower_of(LEAF);
+    static constexpr uint32_t MAXF = (MAXM + SPLIT - 1) / SPLIT;
+    static constexpr bool WIDE = MAXF > 4;
+    static constexpr uint64_t SEED_INDEX = STAGE == kStageUpper ? 17 : 18;
+};
+
+template <int LEAF, int STAGE, bool FULL, bool WIDE>
+__device__ __forceinline__ uint32_t aggr_window(const uint64_t *sk, uint32_t m, uint32_t fan, uint64_t bx,
+                                                uint32_t tlo, uint32_t thi) {
+    using C = AggrCfg<LEAF, STAGE>;
+    constexpr int S = kAggrSeedsPerLane;
+    uint32_t lo[S], hi[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) lo[s] = hi[s] = 0;
+    for (uint32_t i = 0; i < m; ++i) {
+        const uint64_t t = sk[i] + bx;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const uint32_t h = hash16(t + 32u * s);
+            const uint32_t p = FULL ? (h * fan) >> 16 : ((h * m) >> 16) / C::SPLIT;
+            if (WIDE) {
+                lo[s] += shl_clamp(1u, 8 * p);
+                hi[s] += shl_clamp(1u, 8 * p - 32);
+            } else {
+                lo[s] += 1u << (8 * p);
+            }
+        }
+    }
+    uint32_t best = 0xFFFFFFFFu;
+#pragma unroll
+    for (int s = S - 1; s >= 0; --s)
+        if (lo[s] == tlo && (!WIDE || hi[s] == thi)) best = (threadIdx.x & 31) + 32u * s;
+    return best;
+}
+
+template <int LEAF, int STAGE>
+__global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
+    using C = AggrCfg<LEAF, STAGE>;
+    constexpr uint32_t W = 32 * kAggrSeedsPerLane;
+    extern __shared__ uint64_t smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint64_t *sk = smem + warp * C::MAXM;
+    const uint32_t gw = blockIdx.x * kWarpsPerCta + warp;
+    const uint32_t count = c.stage_info[STAGE];
+    const uint32_t base = c.stage_info[kNumStages + STAGE];
+    const uint64_t seed = start_seed(C::SEED_INDEX);
+    uint32_t rng = gw * 2654435761u + 12345u;
+    uint32_t node = kEmpty, m = 0, fan = 0, tlo = 0, thi = 0;
+    bool owner = false, full = false;
+    uint64_t budget = 0;
+    for (;;) {
+        if (node == kEmpty) {
+            if (status_code(c.status)) break;
+            uint32_t f = 0;
+            if (lane == 0) f = atomicAdd(&c.sched[STAGE], 1u);
+            f = __shfl_sync(0xffffffffu, f, 0);
+            if (f < count) {
+                node = c.lists[base + f];
+                owner = true;
+                if (lane == 0) c.slots[gw] = node;
+            } else {
+                owner = false;
+                rng = rng * 1664525u + 1013904223u;
+                node = find_help(c, rng % c.nslots);
+                if (node == kEmpty) break;
+            }
+            const uint32_t start = c.nodes.start[node];
+            m = c.nodes.size[node];
+            __syncwarp();
+            for (uint32_t i = lane; i < m; i += 32) sk[i] = c.keys[start + i];
+            __syncwarp();
+            fan = uint16_t(m + C::SPLIT - 1) / C::SPLIT;
+            full = m == fan * C::SPLIT;
+            tlo = thi = 0;
+            for (uint32_t j = 0; j < 8 && j < fan; ++j) {
+                const uint32_t t = j + 1 < fan ? C::SPLIT : m - (fan - 1) * C::SPLIT;
+                if (j < 4) tlo |= t << (8 * j);
+                else thi |= t << (8 * (j - 4));
+            }
+            budget = budget_for(c, m);
+        }
+        uint32_t w = 0;
+        if (lane == 0) w = atomicAdd(&c.nodes.next_win[node], 1u);
+        w = __shfl_sync(0xffffffffu, w, 0);
+        const uint64_t x0 = (uint64_t)w * W;
+        const uint64_t best = vload64(&c.nodes.seed[node]);
+        if (x0 >= best || x0 >= budget) {
+            if (x0 < best && lane == 0) atomicMin((unsigned long long *)&c.nodes.seed[node], (unsigned long long)kSeedFailed);
+            if (owner && lane == 0) c.slots[gw] = kEmpty;
+            node = kEmpty;
+            continue;
+        }
+        const uint64_t bx = seed + x0 + lane;
+        uint32_t off;
+        if (C::WIDE) {
+            off = full ? aggr_window<LEAF, STAGE, true, C::WIDE>(sk, m, fan, bx, tlo, thi)
+                       : aggr_window<LEAF, STAGE, false, C::WIDE>(sk, m, fan, bx, tlo, thi);
+        } else {
+            off = full ? aggr_window<LEAF, STAGE, true, false>(sk, m, fan, bx, tlo, thi)
+                       : aggr_window<LEAF, STAGE, false, false>(sk, m, fan, bx, tlo, thi);
+        }
+        off = __reduce_min_sync(0xffffffffu, off);
+        if (off != 0xFFFFFFFFu && lane == 0)
+            atomicMin((unsigned long long *)&c.nodes.seed[node], (unsigned long long)(x0 + off));
+    }
+}
+
+// Stable fanout-way partition of aggregation nodes once their stage is complete
+// (SIMDRecSplit.hpp:395-412), one warp per node.
+template <int LEAF, int STAGE>
+__global__ void __launch_bounds__(kThreads) k_partition_aggr(SearchCtx c) {
+    using C = AggrCfg<LEAF, STAGE>;
+    extern __shared__ uint64_t smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint64_t *sk = smem + warp * C::MAXM;
+    const uint32_t count = c.stage_info[STAGE];
+    const uint32_t base = c.stage_info[kNumStages + STAGE];
+    const uint64_t seed = start_seed(C::SEED_INDEX);
+    const uint32_t nwarps = gridDim.x * kWarpsPerCta;
+    for (uint32_t li = blockIdx.x * kWarpsPerCta + warp; li < count; li += nwarps) {
+        const uint32_t id = c.lists[base + li];
+        const uint64_t x = c.nodes.seed[id];
+        if (x >= kSeedFailed) {
+            if (lane == 0) set_error(c.status, RSB_ERR_SEARCH_BUDGET, id);
+            continue;
+        }
+        const uint32_t start = c.nodes.start[id];
+        const uint32_t m = c.nodes.size[id];
+        for (uint32_t i = lane; i < m; i += 32) sk[i] = c.keys[start + i];
+        __syncwarp();
+        const uint32_t fan = uint16_t(m + C::SPLIT - 1) / C::SPLIT;
+        uint32_t cur[C::MAXF];
+#pragma unroll
+        for (uint32_t j = 0; j < C::MAXF; ++j) cur[j] = j * C::SPLIT;
+        const uint64_t sx = seed + x;
+        for (uint32_t c0 = 0; c0 < m; c0 += 32) {
+            const uint32_t i = c0 + lane;
+            const bool valid = i < m;
+            const uint64_t k = valid ? sk[i] : 0;
+            const uint32_t p = valid ? remap16(k + sx, m) / C::SPLIT : 0xFFu;
+            uint32_t dst = 0;
+#pragma unroll
+            for (uint32_t j = 0; j < C::MAXF; ++j) {
+                if (j < fan) {
+                    const unsigned b = __ballot_sync(0xffffffffu, p == j);
+                    if (p == j) dst = cur[j] + __popc(b & ((1u << lane) - 1));
+                    cur[j] += __popc(b);
+                }
+            }
+            if (valid) c.keys[start + dst] = k;
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Leaves. Rotation leaves (m == LEAF): left = even `second`, right = odd; for base b the
+// encoded seed is b*LEAF + r with r the least left rotation of the right mask that fills
+// the complement of the left mask. Brute-force leaves: the first x whose m bit positions
+// are all distinct.
+// ---------------------------------------------------------------------------------------
+constexpr int kLeafSeedsPerLane = 4;
+
+template <int LEAF>
+__device__ __forceinline__ uint32_t rotl_leaf(uint32_t v, uint32_t r) {
+    constexpr uint32_t full = (LEAF == 32) ? 0xFFFFFFFFu : ((1u << LEAF) - 1);
+    return ((v << r) | (v >> (LEAF - r))) & full;
+}
+
+template <int LEAF, bool ROT>
+__global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
+    constexpr int STAGE = ROT ? kStageLeafRot : kStageLeafBF;
+    constexpr int S = kLeafSeedsPerLane;
+    constexpr uint32_t W = 32 * S;
+    __shared__ uint64_t skeys[kWarpsPerCta][LEAF];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint64_t *sk = skeys[warp];
+    const uint32_t gw = blockIdx.x * kWarpsPerCta + warp;
+    const uint32_t count = c.stage_info[STAGE];
+    const uint32_t base = c.stage_info[kNumStages + STAGE];
+    const uint64_t seed = start_seed(kNumStartSeeds - 1);
+    uint32_t rng = gw * 2654435761u + 777u;
+    uint32_t node = kEmpty, m = 0, nl = 0;
+    bool owner = false;
+    uint64_t budget = 0;
+    for (;;) {
+        if (node == kEmpty) {
+            if (status_code(c.status)) break;
+            uint32_t f = 0;
+            if (lane == 0) f = atomicAdd(&c.sched[STAGE], 1u);
+            f = __shfl_sync(0xffffffffu, f, 0);
+            if (f < count) {
+                node = c.lists[base + f];
+                owner = true;
+                if (lane == 0) c.slots[gw] = node;
+            } else {
+                owner = false;
+                rng = rng * 1664525u + 1013904223u;
+                node = find_help(c, rng % c.nslots);
+                if (node == kEmpty) break;
+            }
+            const uint32_t start = c.nodes.start[node];
+            m = c.nodes.size[node];
+            const uint64_t k = lane < (int)m ? c.keys[start + lane] : 0;
+            __syncwarp();
+            if (ROT) {
+                const unsigned even = __ballot_sync(0xffffffffu, lane < (int)m && (k & 1) == 0);
+                const unsigned odd = __ballot_sync(0xffffffffu, lane < (int)m && (k & 1) == 1);
+                nl = __popc(even);
+                const unsigned below = (1u << lane) - 1;
+                if (lane < (int)m) sk[(k & 1) ? nl + __popc(odd & below) : __popc(even & below)] = k;
+            } else {
+                if (lane < (int)m) sk[lane] = k;
+            }
+            __syncwarp();
+            budget = budget_for(c, m);
+        }
+        uint32_t w = 0;
+        if (lane == 0) w = atomicAdd(&c.nodes.next_win[node], 1u);
+        w = __shfl_sync(0xffffffffu, w, 0);
+        const uint64_t x0 = (uint64_t)w * W;                   // first base (ROT) or seed of the window
+        const uint64_t enc0 = ROT ? x0 * LEAF : x0;            // first encoded seed of the window
+        const uint64_t best = vload64(&c.nodes.seed[node]);
+        if (enc0 >= best || enc0 >= budget) {
+            if (enc0 < best && lane == 0) atomicMin((unsigned long long *)&c.nodes.seed[node], (unsigned long long)kSeedFailed);
+            if (owner && lane == 0) c.slots[gw] = kEmpty;
+            node = kEmpty;
+            continue;
+        }
+        uint32_t off = 0xFFFFFFFFu;
+        if (ROT) {
+            constexpr uint32_t full = (1u << LEAF) - 1;
+#pragma unroll
+            for (int s = S - 1; s >= 0; --s) {
+                const uint64_t b = x0 + lane + 32u * s;
+                const uint64_t bx = seed + b * LEAF;
+                uint32_t ml = 0, mr = 0;
+                for (uint32_t i = 0; i < nl; ++i) ml |= 1u << remap16(sk[i] + bx, LEAF);
+                for (uint32_t i = nl; i < (uint32_t)LEAF; ++i) mr |= 1u << remap16(sk[i] + bx, LEAF);
+                if (__popc(ml) == (int)nl && __popc(mr) == LEAF - (int)nl) {
+                    const uint32_t want = full & ~ml;
+                    for (uint32_t r = 0; r < (uint32_t)LEAF; ++r) {
+                        if (rotl_leaf<LEAF>(mr, r) == want) {
+                            off = (lane + 32u * s) * LEAF + r;
+                            break;
+                        }
+                    }
+                }
+            }
+        } else {
+            const uint32_t full = (1u << m) - 1;
+#pragma unroll
+            for (int s = S - 1; s >= 0; --s) {
+                const uint64_t bx = seed + x0 + lane + 32u * s;
+                uint32_t mask = 0;
+                for (uint32_t i = 0; i < m; ++i) mask |= 1u << remap16(sk[i] + bx, m);
+                if (mask == full) off = lane + 32u * s;
+            }
+        }
+        off = __reduce_min_sync(0xffffffffu, off);
+        if (off != 0xFFFFFFFFu && lane == 0)
+            atomicMin((unsigned long long *)&c.nodes.seed[node], (unsigned long long)(enc0 + off));
+    }
+}
+
+// ---- host-side dispatch -------------------------------------------------------------
+
+template <typename K>
+int persistent_grid(K kernel, size_t smem, int num_sms) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, smem);
+    if (per_sm < 1) per_sm = 1;
+    return per_sm * num_sms;
+}
+
+template <int LEAF>
+void run_aggr(const SearchCtx &c, int stage, cudaStream_t st) {
+    if (stage == kStageUpper) {
+        using C = AggrCfg<LEAF, kStageUpper>;
+        const size_t smem = kWarpsPerCta * C::MAXM * sizeof(uint64_t);
+        auto k = k_search_aggr<LEAF, kStageUpper>;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int g = persistent_grid(k, smem, c.num_sms);
+        g = min(g, (int)(c.nslots / kWarpsPerCta));
+        SearchCtx cc = c;
+        cc.nslots = g * kWarpsPerCta;
+        k<<<g, kThreads, smem, st>>>(cc);
+    } else {
+        using C = AggrCfg<LEAF, kStageLower>;
+        const size_t smem = kWarpsPerCta * C::MAXM * sizeof(uint64_t);
+        auto k = k_search_aggr<LEAF, kStageLower>;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int g = persistent_grid(k, smem, c.num_sms);
+        g = min(g, (int)(c.nslots / kWarpsPerCta));
+        SearchCtx cc = c;
+        cc.nslots = g * kWarpsPerCta;
+        k<<<g, kThreads, smem, st>>>(cc);
+    }
+}
+
+template <int LEAF>
+void run_partition(const SearchCtx &c, int stage, cudaStream_t st) {
+    if (stage == kStageUpper) {
+        using C = AggrCfg<LEAF, kStageUpper>;
+        const size_t smem = kWarpsPerCta * C::MAXM * sizeof(uint64_t);
+        auto k = k_partition_aggr<LEAF, kStageUpper>;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k<<<persistent_grid(k, smem, c.num_sms), kThreads, smem, st>>>(c);
+    } else {
+        using C = AggrCfg<LEAF, kStageLower>;
+        const size_t smem = kWarpsPerCta * C::MAXM * sizeof(uint64_t);
+        auto k = k_partition_aggr<LEAF, kStageLower>;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k<<<persistent_grid(k, smem, c.num_sms), kThreads, smem, st>>>(c);
+    }
+}
+
+template <int LEAF>
+void run_leaves(const SearchCtx &c, int stage, cudaStream_t st) {
+    SearchCtx cc = c;
+    if (stage == kStageLeafRot) {
+        auto k = k_search_leaf<LEAF, true>;
+        int g = min(persistent_grid(k, 0, c.num_sms), (int)(c.nslots / kWarpsPerCta));
+        cc.nslots = g * kWarpsPerCta;
+        k<<<g, kThreads, 0, st>>>(cc);
+    } else {
+        auto k = k_search_leaf<LEAF, false>;
+        int g = min(persistent_grid(k, 0, c.num_sms), (int)(c.nslots / kWarpsPerCta));
+        cc.nslots = g * kWarpsPerCta;
+        k<<<g, kThreads, 0, st>>>(cc);
+    }
+}
+
+#define RSB_LEAF_SWITCH(leaf, FN, ...)          \
+    switch (leaf) {                             \
+        case 2: FN<2>(__VA_ARGS__); break;      \
+        case 3: FN<3>(__VA_ARGS__); break;      \
+        case 4: FN<4>(__VA_ARGS__); break;      \
+        case 5: FN<5>(__VA_ARGS__); break;      \
+        case 6: FN<6>(__VA_ARGS__); break;      \
+        case 7: FN<7>(__VA_ARGS__); break;      \
+        case 8: FN<8>(__VA_ARGS__); break;      \
+        case 9: FN<9>(__VA_ARGS__); break;      \
+        case 10: FN<10>(__VA_ARGS__); break;    \
+        case 11: FN<11>(__VA_ARGS__); break;    \
+        case 12: FN<12>(__VA_ARGS__); break;    \
+        case 13: FN<13>(__VA_ARGS__); break;    \
+        case 14: FN<14>(__VA_ARGS__); break;    \
+        case 15: FN<15>(__VA_ARGS__); break;    \
+        case 16: FN<16>(__VA_ARGS__); break;    \
+        case 17: FN<17>(__VA_ARGS__); break;    \
+        case 18: FN<18>(__VA_ARGS__); break;    \
+        case 19: FN<19>(__VA_ARGS__); break;    \
+        case 20: FN<20>(__VA_ARGS__); break;    \
+        case 21: FN<21>(__VA_ARGS__); break;    \
+        case 22: FN<22>(__VA_ARGS__); break;    \
+        case 23: FN<23>(__VA_ARGS__); break;    \
+        case 24: FN<24>(__VA_ARGS__); break;    \
+        default: break;                         \
+    }
+
+}  // namespace
+
+uint32_t search_slots_needed(int num_sms) { return (uint32_t)num_sms * 64u; }  // 64 resident warps per SM at most
+
+bool shape_matches_kernels(const Shape &s) { return s.lower == lower_of((int)s.leaf) && s.upper == upper_of((int)s.leaf); }
+
+void search_higher(const SearchCtx &c, int depth, cudaStream_t st) {
+    const size_t smem = kMaxBucketSize * sizeof(uint64_t);
+    cudaFuncSetAttribute(k_search_higher, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_search_higher<<<persistent_grid(k_search_higher, smem, c.num_sms), kThreads, smem, st>>>(c, depth);
+}
+
+void search_aggr(const SearchCtx &c, int stage, cudaStream_t st) { RSB_LEAF_SWITCH(c.sh.leaf, run_aggr, c, stage, st); }
+void partition_aggr(const SearchCtx &c, int stage, cudaStream_t st) { RSB_LEAF_SWITCH(c.sh.leaf, run_partition, c, stage, st); }
+void search_leaves(const SearchCtx &c, int stage, cudaStream_t st) { RSB_LEAF_SWITCH(c.sh.leaf, run_leaves, c, stage, st); }
+
+}  // namespace rsb

@@ -1,0 +1,146 @@
+/*
+ * rsb.h — C ABI of the B200-native RecSplit construction engine (librsb.so).
+ *
+ * This is the drop-in boundary for the construction path of ByteHamster/GpuRecSplit.
+ * Every entry point takes plain pointers and sizes; no C++ or CUDA types cross it
+ * (streams are passed as void*). The C++ class in include/rsb/GPURecSplit.hpp wraps
+ * these calls behind the reference's GPURecSplit<LEAF_SIZE, AT, ROTATE> interface.
+ *
+ * Reference interfaces are cited as path:line within the GpuRecSplit project.
+ *
+ * Ownership: the caller owns every input buffer; the library owns engines and handles
+ * and frees them in rsb_engine_destroy / rsb_free. The library never calls exit(),
+ * abort() or cudaDeviceReset(); every failure is returned as an rsb_status.
+ * Threading: an engine may be used by one host thread at a time; handles are immutable
+ * after construction and may be queried concurrently.
+ */
+#ifndef RSB_H_
+#define RSB_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum rsb_status {
+    RSB_OK = 0,
+    RSB_ERR_BAD_ARG = 1,          /* invalid leaf size, bucket size, pointer or flag */
+    RSB_ERR_CUDA = 2,             /* a CUDA runtime call failed */
+    RSB_ERR_OOM = 3,              /* device or host allocation failed */
+    RSB_ERR_DUPLICATE_KEY = 4,    /* two keys share a bucket and the same second half; the
+                                     reference loops forever here (GPURecSplit.cuh:436) */
+    RSB_ERR_SEARCH_BUDGET = 5,    /* a seed search exceeded its candidate budget */
+    RSB_ERR_BUCKET_TOO_LARGE = 6, /* a bucket holds >= 3000 keys (AbstractParallelRecSplit.hpp:60;
+                                     the reference throws std::out_of_range, GPURecSplit.cuh:682) */
+    RSB_ERR_TIMEOUT = 7,          /* a bounded device wait gave up */
+    RSB_ERR_FORMAT = 8,           /* malformed serialized input or leaf-size mismatch
+                                     (the reference abort()s, GPURecSplit.cuh:831-833) */
+    RSB_ERR_INTERNAL = 9,
+    RSB_ERR_NO_DEVICE = 10        /* no CUDA device or the kernels do not match it */
+} rsb_status;
+
+/* Build flags. */
+#define RSB_ROTATE 1u          /* USE_BIJECTIONS_ROTATE template parameter (reference default true) */
+#define RSB_KEYS_ON_DEVICE 2u  /* key pointers are device memory; otherwise host memory */
+#define RSB_DEVICE_ONLY 4u     /* keep the result on the device; the host copy is made lazily */
+#define RSB_KEEP_SEEDS 8u      /* keep the DFS seed stream for rsb_seeds() */
+
+/* 128-bit key hash: util/Hash128.h:14-23 (hash128_t{first, second}). */
+typedef struct rsb_hash128 {
+    uint64_t first, second;
+} rsb_hash128;
+
+typedef struct rsb_engine rsb_engine; /* device context: stream, cached scratch, tables */
+typedef struct rsb_mphf rsb_mphf;     /* one built minimal perfect hash function */
+
+/* Per-build measurements (device time from CUDA events on the engine stream). */
+typedef struct rsb_stats {
+    uint64_t keys;
+    uint64_t buckets;
+    uint64_t nodes;                /* seeds in the descriptor stream */
+    uint64_t nodes_per_stage[21];  /* 0..16 fanout-2 depth d, 17 upper aggr, 18 lower aggr, 19 rotation leaves, 20 other leaves */
+    uint64_t evals_alg;            /* sum over nodes of (trials up to the found seed) * node size */
+    uint64_t descriptor_bits;      /* Golomb-Rice stream length without the sentinel */
+    double ms_total;               /* whole build on the device */
+    double ms_partition;           /* hashing, bucket histogram/scan/scatter, per-bucket sort */
+    double ms_search[21];          /* per search stage */
+    double ms_encode;              /* Rice + Elias-Fano */
+} rsb_stats;
+
+/* ---- engine ------------------------------------------------------------------------ */
+
+/* Creates an engine on `device` (an int CUDA ordinal). `stream` (a cudaStream_t, may be
+ * NULL for a private stream) is where all work of this engine is enqueued. */
+rsb_status rsb_engine_create(int device, void *stream, rsb_engine **out);
+rsb_status rsb_engine_destroy(rsb_engine *engine);
+/* Candidate budget of every seed search: 2^(g(m) + shift) seeds, at least 2^16 (default
+ * shift 10). Exceeding it ends the build with RSB_ERR_SEARCH_BUDGET instead of looping. */
+rsb_status rsb_engine_set_budget(rsb_engine *engine, uint32_t shift, uint64_t min_candidates);
+
+/* ---- construction ------------------------------------------------------------------ */
+
+/* Replaces GPURecSplit(vector<hash128_t>& keys, size_t bucket_size, int numThreads),
+ * GPURecSplit.cuh:484-489 (same for SIMDRecSplit.hpp:228-232). The caller's keys are
+ * not modified (the reference sorts them in place, AbstractParallelRecSplit.hpp:344). */
+rsb_status rsb_build_hash128(rsb_engine *engine, const rsb_hash128 *keys, uint64_t n, uint64_t bucket_size,
+                             uint32_t leaf_size, uint32_t flags, rsb_mphf **out);
+
+/* Replaces GPURecSplit(const vector<string>& keys, size_t bucket_size, int numThreads),
+ * GPURecSplit.cuh:443-472: key i is bytes[offsets[i] .. offsets[i+1]); hashed on the
+ * device with SpookyHash V2 (seed 0), first = h1, second = h0 (util/Hash128.h:32-36). */
+rsb_status rsb_build_strings(rsb_engine *engine, const uint8_t *bytes, const uint64_t *offsets, uint64_t n,
+                             uint64_t bucket_size, uint32_t leaf_size, uint32_t flags, rsb_mphf **out);
+
+/* 64-bit integer keys (no reference counterpart: the reference benchmarks feed random
+ * hash128 values, benchmark/benchmark_construction.hpp:54-58). Each key k is mixed to
+ * first = fmix64(k) (MurmurHash3), second = stafford13(k + 0x9e3779b97f4a7c15). */
+rsb_status rsb_build_u64(rsb_engine *engine, const uint64_t *keys, uint64_t n, uint64_t bucket_size,
+                         uint32_t leaf_size, uint32_t flags, rsb_mphf **out);
+
+/* ---- queries and accessors --------------------------------------------------------- */
+
+/* Replaces size_t operator()(const hash128_t&), AbstractParallelRecSplit.hpp:409-466
+ * (host evaluation; keys and out are host memory). */
+rsb_status rsb_query_hash128(rsb_mphf *mphf, const rsb_hash128 *keys, uint64_t n, uint64_t *out);
+/* Replaces size_t operator()(const string&), AbstractParallelRecSplit.hpp:473. */
+rsb_status rsb_query_strings(rsb_mphf *mphf, const uint8_t *bytes, const uint64_t *offsets, uint64_t n,
+                             uint64_t *out);
+/* Device evaluation of operator() for many keys (keys and out are device memory, work is
+ * enqueued on the engine stream and completed before return). */
+rsb_status rsb_query_device(rsb_engine *engine, rsb_mphf *mphf, const rsb_hash128 *keys, uint64_t n,
+                            uint64_t *out);
+
+/* Replaces size_t getBits(), AbstractParallelRecSplit.hpp:476-478. */
+rsb_status rsb_get_bits(rsb_mphf *mphf, uint64_t *bits);
+/* Replaces operator<<, GPURecSplit.cuh:817-825. With buf == NULL only *len is set. */
+rsb_status rsb_serialize(rsb_mphf *mphf, uint8_t *buf, size_t *len);
+/* Replaces operator>>, GPURecSplit.cuh:827-841; a leaf size other than `leaf_size`
+ * returns RSB_ERR_FORMAT instead of abort(). `flags` carries RSB_ROTATE. */
+rsb_status rsb_deserialize(const uint8_t *buf, size_t len, uint32_t leaf_size, uint32_t flags, rsb_mphf **out);
+/* Seeds in descriptor (DFS pre-order) order with the size of each node; for parity
+ * debugging (no reference counterpart). With seeds == NULL only *count is set. */
+rsb_status rsb_seeds(rsb_mphf *mphf, uint64_t *seeds, uint32_t *sizes, size_t *count);
+rsb_status rsb_get_stats(rsb_mphf *mphf, rsb_stats *stats);
+rsb_status rsb_free(rsb_mphf *mphf);
+
+/* ---- hashing only (parity checks of the key mixers) --------------------------------- */
+rsb_status rsb_hash_strings(rsb_engine *engine, const uint8_t *bytes, const uint64_t *offsets, uint64_t n,
+                            uint32_t flags, rsb_hash128 *out);
+rsb_status rsb_hash_u64(rsb_engine *engine, const uint64_t *keys, uint64_t n, uint32_t flags, rsb_hash128 *out);
+
+/* Golomb-Rice table of the engine for one leaf size (3000 entries), the table generated by
+ * fill_golomb_rice<LEAF_SIZE>() (AbstractParallelRecSplit.hpp:191-227) and shipped as
+ * golombRiceMemo.hpp. Host-only; needs no device. */
+rsb_status rsb_golomb_memo(uint32_t leaf_size, uint32_t *out);
+
+const char *rsb_strerror(rsb_status status);
+/* Library version string. */
+const char *rsb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RSB_H_ */
