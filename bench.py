@@ -1,0 +1,341 @@
+#!/usr/bin/env python
+"""Benchmark of RecSplit construction on B200: build ns/key at l=16, b=2000, n=5M.
+
+One step = one complete construction (hash to 128 bits, bucket partition, every seed
+search, Golomb-Rice + double Elias-Fano encoding) of n=5,000,000 uniform random 64-bit
+keys (splitmix64, seed 42 + rank) with leaf size 16, bucket size 2000 and rotation fitting.
+
+  value   device time of a build from keys resident in HBM (CUDA events on the engine
+          stream, L2 flushed by a 256 MiB write before every timed step), ns per key
+  e2e     the same build through the public API from pinned host keys: host->device copy
+          of the keys, construction, device->host copy of the built function and its
+          serialization, all inside the timed region
+  roofline  the dominant search kernel's algorithmic evaluation rate (sum over its nodes
+          of candidates x node size / its device time) against the device's measured
+          remixAndRemap32 evaluation ceiling (rsb_probe_eval_rate)
+  cpu_baseline  the scalar CPU oracle (restatement of SIMDRecSplit, all host cores) on a
+          bounded sample of the same workload
+
+`--impl reference` times only the CPU implementation of the path (the oracle port; the
+reference's own SIMDRecSplit cannot be compiled here: its submodules are absent).
+
+Multi-GPU (torchrun): every rank builds its own 5M-key set (weak scaling, no data-path
+collective); the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import datetime
+import hashlib
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "build ns/key (l=16,b=2000,n=5M)"
+UNIT = "ns/key"
+N_KEYS = 5_000_000
+LEAF = 16
+BUCKET = 2000
+SEED = 42
+PUBLISHED_NS_PER_KEY = 1000.0  # GpuRecSplit, l=16 b=2000 n=5M: 1.0 us/object (README.md:18)
+GOLDEN = os.path.join(ROOT, "tests", "golden", "golden_builds.json")
+PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "traffic.json")
+
+
+def splitmix64_keys(seed: int, n: int) -> np.ndarray:
+    """n outputs of splitmix64 (Steele, Lea, Flood 2014) started at `seed`."""
+    with np.errstate(over="ignore"):
+        i = np.arange(1, n + 1, dtype=np.uint64)
+        z = np.uint64(seed) + i * np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+def workload_config(n: int, world: int) -> dict:
+    return {
+        "workload": f"u64 keys n={n} (splitmix64 seed 42+rank) hashed to 128 bits (fmix64 / stafford13), "
+                    f"RecSplit l={LEAF} b={BUCKET} with rotation fitting",
+        "n": n, "leaf": LEAF, "bucket": BUCKET, "nbuckets": (n + BUCKET - 1) // BUCKET,
+        "l2": "flushed before every timed step (256 MiB device write)",
+        "parallelism": f"replicas x{world} (independent key sets per GPU)" if world > 1 else "single GPU",
+    }
+
+
+# ---------------------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=10)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self) -> dict:
+        rows = [r for r in csv.reader(io.StringIO(getattr(self, "out", ""))) if len(r) >= 9]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for k, name in enumerate(names):
+                if r[5 + k].strip().lower() == "active":
+                    reasons.add(name)
+        loaded = [s for s in sm if s > 0.5 * max(sm)] if sm else []
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------------------
+# CPU side (oracle) — the timed CPU baseline and the reference arm
+# ---------------------------------------------------------------------------------------
+def cpu_sample(buckets: int, seed: int = SEED):
+    """Keys of a bounded sample with the bench workload's shape: `buckets` buckets of b=2000."""
+    import oracle
+    n = buckets * BUCKET
+    keys = oracle.hash_u64(splitmix64_keys(seed, n))
+    return keys, n
+
+
+def time_cpu_oracle(buckets: int, threads: int) -> dict:
+    import oracle
+    keys, n = cpu_sample(buckets)
+    t0 = time.perf_counter()
+    res = oracle.build_mphf(keys, LEAF, BUCKET, True, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": dt * 1e9 / n, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{buckets} buckets of b={BUCKET} ({n} keys, same key stream and l={LEAF}) out of the "
+                      f"{(N_KEYS + BUCKET - 1) // BUCKET}-bucket workload; scalar oracle, {threads} threads",
+            "seconds": dt, "bits_per_key": oracle.get_bits(res.bytes) / n}
+
+
+def run_reference(args, rank: int, world: int) -> None:
+    if rank != 0:
+        return
+    import oracle
+    oracle.build()
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        time_cpu_oracle(args.ref_buckets, threads)
+    vals = [time_cpu_oracle(args.ref_buckets, threads) for _ in range(args.steps)]
+    v = statistics.mean(x["value"] for x in vals)
+    line = {
+        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": statistics.mean(x["seconds"] for x in vals) * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": v / PUBLISHED_NS_PER_KEY, "dtype": "u64", "data": "synthetic",
+        "impl": "reference",
+        "config": workload_config(N_KEYS, world) | {"cpu_sample_buckets": args.ref_buckets},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": vals[0]["sample"]},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "CPU oracle (scalar restatement of SIMDRecSplit); the reference itself cannot be built here "
+                "(its sux, vectorclass, gcem, ips2ra and SpookyV2 submodules are empty)",
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------------------
+def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
+    import torch
+    import gpurecsplit_b200 as rsb
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    stream = torch.cuda.current_stream()
+    engine = rsb.Engine(local_rank, stream.cuda_stream)
+    n = args.n
+    keys_host = splitmix64_keys(SEED + rank, n)
+    pinned = torch.from_numpy(keys_host.view(np.int64)).pin_memory()
+    keys_dev = pinned.to(f"cuda:{local_rank}")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local_rank}")
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def device_build():
+        return rsb.GPURecSplit.from_device(keys_dev.data_ptr(), n, BUCKET, LEAF, key_type="u64", engine=engine,
+                                           device_only=True)
+
+    # warm-up (also loads the kernels and sizes the engine's scratch)
+    for _ in range(args.warmup):
+        flush.zero_()
+        device_build().close()
+    torch.cuda.synchronize()
+
+    # ---- timed: device-resident builds ----
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stats = []
+    last = None
+    with ClockSampler(local_rank) as clocks:
+        barrier()
+        for i in range(args.steps):
+            flush.zero_()
+            starts[i].record(stream)
+            f = device_build()
+            ends[i].record(stream)
+            stats.append(f.stats())
+            if last is not None:
+                last.close()
+            last = f
+        barrier()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = sum(step_ms)
+    if dist is not None:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = ms_per_step * 1e6 / (n * world)
+
+    # parity of the last timed build with the committed oracle digest
+    parity = None
+    if rank == 0 and os.path.exists(GOLDEN) and n == N_KEYS:
+        g = json.load(open(GOLDEN)).get("u64_n5M_l16_b2000")
+        if g is not None:
+            blob = last.serialize()
+            parity = {"sha256_equals_oracle": hashlib.sha256(blob).hexdigest() == g["sha256"],
+                      "bits_per_key": last.get_bits() / n}
+    bits_per_key = last.get_bits() / n
+    last.close()
+
+    # ---- timed: end to end through the public API from pinned host keys ----
+    e2e_steps = max(1, min(args.steps, 3))
+    e2e_ms = []
+    d2h_bytes = 0
+    host_keys = pinned.numpy().view(np.uint64)
+    for i in range(e2e_steps + 1):
+        flush.zero_()
+        barrier()
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        f = rsb.GPURecSplit(host_keys, bucket_size=BUCKET, leaf_size=LEAF, key_type="u64", engine=engine)
+        blob = f.serialize()
+        e.record(stream)
+        e.synchronize()
+        if i > 0:  # the first one is a warm-up of the host paths
+            e2e_ms.append(s.elapsed_time(e))
+        # structure words copied back (the 14 serialization header words are not copied) plus
+        # the status word, encoder parameters and stage counts read at the end of the build
+        d2h_bytes = len(blob) - 8 * 14 + 16 + 8 * 36 + 4 * 21
+        f.close()
+    e2e_total = sum(e2e_ms)
+    if dist is not None:
+        t = torch.tensor([e2e_total], dtype=torch.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = e2e_total / e2e_steps * 1e6 / (n * world)
+
+    if rank == 0:
+        # ---- roofline of the dominant search kernel ----
+        st = stats[-1]
+        ms_search = st["ms_search"]
+        dom = max(range(21), key=lambda s: ms_search[s])
+        names = {17: "upper aggregation (k_search_aggr<16,17>)", 18: "lower aggregation (k_search_aggr<16,18>)",
+                 19: "rotation leaves (k_search_leaf<16,true>)", 20: "brute-force leaves (k_search_leaf<16,false>)"}
+        dom_name = names.get(dom, f"fanout-2 depth {dom} (k_search_higher)")
+        achieved = st["evals_stage"][dom] / (ms_search[dom] * 1e-3) / 1e9
+        peak_rates = [engine.probe_eval_rate()[0] for _ in range(3)]
+        peak = max(peak_rates) / 1e9
+        traffic = None
+        if os.path.exists(PROFILE_TRAFFIC):
+            traffic = json.load(open(PROFILE_TRAFFIC)).get(str(dom))
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            import oracle
+            oracle.build()
+            cpu = time_cpu_oracle(args.cpu_buckets, os.cpu_count() or 1)
+            cpu.pop("seconds", None)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": value / PUBLISHED_NS_PER_KEY, "dtype": "u64", "data": "synthetic",
+            "config": workload_config(n, world),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": d2h_bytes},
+            "roofline": {"bound": "int", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "Geval/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": "rsb_probe_eval_rate: measured remixAndRemap32 evaluation ceiling on this GPU",
+                         "evals": st["evals_stage"][dom], "ms": ms_search[dom]},
+            "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+            "gpu_launches": sum(s["kernel_launches"] for s in stats),
+            "bits_per_key": bits_per_key,
+            "parity": parity,
+            "stage_ms": {"partition": st["ms_partition"], "search": {str(i): round(v, 3) for i, v in
+                                                                     enumerate(ms_search) if v > 0},
+                         "encode": st["ms_encode"], "total": st["ms_total"]},
+            "step_ms": [round(x, 3) for x in step_ms],
+        }
+        print(json.dumps(line), flush=True)
+    engine.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="rsb", choices=["rsb", "reference"])
+    ap.add_argument("--n", type=int, default=N_KEYS)
+    ap.add_argument("--cpu-buckets", type=int, default=48)
+    ap.add_argument("--ref-buckets", type=int, default=24)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_gpu(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -49,6 +49,7 @@ class Stats(ctypes.Structure):
         ("nodes_per_stage", ctypes.c_uint64 * 21), ("evals_alg", ctypes.c_uint64),
         ("descriptor_bits", ctypes.c_uint64), ("ms_total", ctypes.c_double), ("ms_partition", ctypes.c_double),
         ("ms_search", ctypes.c_double * 21), ("ms_encode", ctypes.c_double),
+        ("evals_stage", ctypes.c_uint64 * 21), ("kernel_launches", ctypes.c_uint64),
     ]
 
     def as_dict(self) -> dict:
@@ -57,6 +58,7 @@ class Stats(ctypes.Structure):
             "nodes_per_stage": list(self.nodes_per_stage), "evals_alg": self.evals_alg,
             "descriptor_bits": self.descriptor_bits, "ms_total": self.ms_total,
             "ms_partition": self.ms_partition, "ms_search": list(self.ms_search), "ms_encode": self.ms_encode,
+            "evals_stage": list(self.evals_stage), "kernel_launches": self.kernel_launches,
         }
 
 
@@ -95,6 +97,7 @@ def lib():
             "rsb_strerror": ([i32], ctypes.c_char_p),
             "rsb_version": ([], ctypes.c_char_p),
             "rsb_golomb_memo": ([u32, vp], i32),
+            "rsb_probe_eval_rate": ([vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)], i32),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -135,6 +138,12 @@ class Engine:
 
     def set_budget(self, shift: int, min_candidates: int = 1 << 16) -> None:
         _check(lib().rsb_engine_set_budget(self._h, shift, min_candidates), "rsb_engine_set_budget")
+
+    def probe_eval_rate(self):
+        """(evaluations per second, ms) of the synthetic remixAndRemap32 ceiling kernel."""
+        r, ms = ctypes.c_double(), ctypes.c_double()
+        _check(lib().rsb_probe_eval_rate(self._h, ctypes.byref(r), ctypes.byref(ms)), "rsb_probe_eval_rate")
+        return r.value, ms.value
 
     def close(self) -> None:
         if self._h:

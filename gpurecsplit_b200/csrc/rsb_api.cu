@@ -11,6 +11,7 @@
 // grouping, unpacking and encoding on the host and calls cudaDeviceReset at the end.
 #include <algorithm>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <mutex>
 #include <new>
@@ -200,8 +201,11 @@ rsb_status copy_to_host(rsb_mphf *h, cudaStream_t st) {
 }
 
 // The build proper. keys128 is device memory holding n (first, second) pairs.
+// `hash_keys` (optional) enqueues the key-hashing kernel that produces keys128; it runs
+// after the build's start event so that hashing is part of the measured build.
 rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint64_t bucket_size, uint32_t leaf,
-                        uint32_t flags, rsb_mphf **out, bool keep_seeds) {
+                        uint32_t flags, rsb_mphf **out, bool keep_seeds,
+                        const std::function<void()> &hash_keys = std::function<void()>()) {
     const bool rotate = (flags & RSB_ROTATE) != 0;
     const LeafTables &lt = leaf_tables(leaf, rotate);
     if (!shape_matches_kernels(lt.shape)) return RSB_ERR_INTERNAL;
@@ -278,8 +282,10 @@ rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint
     NodeArrays nodes{e->nstart.p, e->nsize.p, e->nstage.p, e->seed.p, e->nwin.p};
     ScanTmp stmp{e->scan_tmp.p, e->scan_tmp.cap};
     const uint64_t *node_total = e->node_base.p + nb;
+    const uint64_t launches0 = launches_so_far();
 
     RSB_CKH(cudaEventRecord(e->ev[0], st));
+    if (hash_keys) hash_keys();
     RSB_CKH(cudaMemsetAsync(e->status.p, 0, sizeof(DevStatus), st));
     RSB_CKH(cudaMemsetAsync(e->efp.p, 0, sizeof(EfParams), st));
     RSB_CKH(cudaMemsetAsync(e->sched.p, 0, kNumStages * sizeof(uint32_t), st));
@@ -358,6 +364,8 @@ rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint
     S.keys = n;
     S.buckets = nb;
     S.evals_alg = h->ef.evals_alg;
+    for (int s = 0; s < kNumStages; ++s) S.evals_stage[s] = h->ef.evals_stage[s];
+    S.kernel_launches = launches_so_far() - launches0;
     S.descriptor_bits = h->ef.total_bits;
     uint64_t tot = 0;
     for (int s = 0; s < kNumStages; ++s) {
@@ -412,6 +420,22 @@ constexpr uint32_t kKeepSeeds = RSB_KEEP_SEEDS;
 extern "C" {
 
 const char *rsb_version(void) { return "rsb 0.1 (sm_100a)"; }
+
+rsb_status rsb_probe_eval_rate(rsb_engine *e, double *evals_per_second, double *ms) {
+    if (!e || !evals_per_second) return RSB_ERR_BAD_ARG;
+    RSB_CK(cudaSetDevice(e->device));
+    uint64_t evals = 0;
+    RSB_CK(cudaEventRecord(e->ev[0], e->stream));
+    probe_eval_rate(e->num_sms, &evals, e->stream);
+    RSB_CK(cudaGetLastError());
+    RSB_CK(cudaEventRecord(e->ev[1], e->stream));
+    RSB_CK(cudaEventSynchronize(e->ev[1]));
+    const double t = elapsed(e->ev[0], e->ev[1]);
+    if (t <= 0) return RSB_ERR_INTERNAL;
+    *evals_per_second = (double)evals / (t * 1e-3);
+    if (ms) *ms = t;
+    return RSB_OK;
+}
 
 rsb_status rsb_golomb_memo(uint32_t leaf, uint32_t *out) {
     if (leaf < 2 || leaf > (uint32_t)kMaxLeafSize || !out) return RSB_ERR_BAD_ARG;
@@ -533,8 +557,10 @@ rsb_status rsb_build_u64(rsb_engine *e, const uint64_t *keys, uint64_t n, uint64
     }
     s = ensure(e->keys128, 2 * n);
     if (s != RSB_OK) return s;
-    launch_hash_u64(dk, n, e->keys128.p, e->stream);
-    return build_device(e, e->keys128.p, n, bucket_size, leaf, flags, out, (flags & kKeepSeeds) != 0);
+    uint64_t *k128 = e->keys128.p;
+    cudaStream_t st = e->stream;
+    return build_device(e, k128, n, bucket_size, leaf, flags, out, (flags & kKeepSeeds) != 0,
+                        [=] { launch_hash_u64(dk, n, k128, st); });
 }
 
 static rsb_status stage_strings(rsb_engine *e, const uint8_t *bytes, const uint64_t *offsets, uint64_t n, uint32_t flags,
@@ -567,8 +593,10 @@ rsb_status rsb_build_strings(rsb_engine *e, const uint8_t *bytes, const uint64_t
     if (s != RSB_OK) return s;
     s = ensure(e->keys128, 2 * n);
     if (s != RSB_OK) return s;
-    launch_hash_strings(db, doff, n, e->keys128.p, e->stream);
-    return build_device(e, e->keys128.p, n, bucket_size, leaf, flags, out, (flags & kKeepSeeds) != 0);
+    uint64_t *k128 = e->keys128.p;
+    cudaStream_t st = e->stream;
+    return build_device(e, k128, n, bucket_size, leaf, flags, out, (flags & kKeepSeeds) != 0,
+                        [=] { launch_hash_strings(db, doff, n, k128, st); });
 }
 
 rsb_status rsb_hash_strings(rsb_engine *e, const uint8_t *bytes, const uint64_t *offsets, uint64_t n, uint32_t flags,

@@ -115,7 +115,9 @@ __global__ void k_write_rice(const uint64_t *node_base, uint64_t nb, NodeArrays 
 
 __device__ __forceinline__ uint64_t bpk_of(const uint64_t *cum, const uint64_t *pos, uint64_t nb) {
     // DoubleEF.hpp:144, the single floating-point operation of the path (IEEE double).
-    if (cum[nb] == 0) return 0;  // no keys: the reference divides 0 by 0 here
+    // With no keys the reference divides 0 by 0 and converts the NaN to uint64; on its x86-64
+    // build that conversion yields 0x8000000000000000, which is what is stored here.
+    if (cum[nb] == 0) return 1ull << 63;
     return (uint64_t)((double)(1ull << 20) * ((double)pos[nb] / (double)cum[nb]));
 }
 
@@ -209,18 +211,27 @@ __global__ void k_ef_fill(const uint64_t *cum, const uint64_t *pos, uint64_t nb,
     }
 }
 
+// Algorithmic work of the searches: sum over nodes of (candidates up to the found seed) * m,
+// candidates being seeds (splits, brute-force leaves) or rotation bases (rotation leaves).
 __global__ void k_evals(const uint64_t *node_total, NodeArrays nodes, uint32_t leaf, uint32_t rotate, EfParams *ef) {
+    __shared__ unsigned long long s_acc[kNumStages];
+    for (int s = threadIdx.x; s < kNumStages; s += blockDim.x) s_acc[s] = 0;
+    __syncthreads();
     const uint64_t n = *node_total;
-    uint64_t acc = 0;
     for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t x = nodes.seed[j];
         const uint32_t m = nodes.size[j];
         if (x >= kSeedFailed) continue;
         const uint64_t trials = (rotate && m == leaf) ? x / leaf + 1 : x + 1;
-        acc += trials * m;
+        atomicAdd(&s_acc[nodes.stage[j]], (unsigned long long)(trials * m));
     }
-    acc = warp_sum64(acc);
-    if ((threadIdx.x & 31) == 0 && acc) atomicAdd((unsigned long long *)&ef->evals_alg, (unsigned long long)acc);
+    __syncthreads();
+    for (int s = threadIdx.x; s < kNumStages; s += blockDim.x) {
+        if (s_acc[s]) {
+            atomicAdd((unsigned long long *)&ef->evals_stage[s], s_acc[s]);
+            atomicAdd((unsigned long long *)&ef->evals_alg, s_acc[s]);
+        }
+    }
 }
 
 int grid_for(uint64_t n, int threads, int cap) {
@@ -235,6 +246,7 @@ int grid_for(uint64_t n, int threads, int cap) {
 void launch_bucket_bits(const uint64_t *node_base, uint64_t nb, NodeArrays nodes, DevTables tab, uint32_t *bits,
                         uint32_t *fixed_bits, DevStatus *status, cudaStream_t st) {
     k_bucket_bits<<<grid_for(nb * 32, 256, 148 * 8), 256, 0, st>>>(node_base, nb, nodes, tab, bits, fixed_bits, status);
+    count_launches(1);
 }
 
 void launch_write_rice(const uint64_t *node_base, uint64_t nb, NodeArrays nodes, DevTables tab, const uint64_t *pos_acc,
@@ -242,6 +254,7 @@ void launch_write_rice(const uint64_t *node_base, uint64_t nb, NodeArrays nodes,
                        DevStatus *status, cudaStream_t st) {
     k_write_rice<<<grid_for(nb * 32, 256, 148 * 8), 256, 0, st>>>(node_base, nb, nodes, tab, pos_acc, fixed_bits, desc,
                                                                    desc_cap_words, ef, status);
+    count_launches(1);
 }
 
 void launch_ef_build(const uint64_t *cum, const uint64_t *pos, uint64_t nb, uint64_t /*keys*/, EfParams *ef,
@@ -251,11 +264,13 @@ void launch_ef_build(const uint64_t *cum, const uint64_t *pos, uint64_t nb, uint
     k_ef_reduce<<<grid_for(nb, 256, 148 * 4), 256, 0, st>>>(cum, pos, nb, ef);
     k_ef_params<<<1, 32, 0, st>>>(cum, pos, nb, ef, lower_cap, cum_cap, pos_cap, jump_cap, status);
     k_ef_fill<<<grid_for(nb + 1, 256, 148 * 8), 256, 0, st>>>(cum, pos, nb, ef, lower, upper_cum, upper_pos, jump, status);
+    count_launches(4);
 }
 
 void launch_evals(const uint64_t *node_total, NodeArrays nodes, uint32_t leaf, uint32_t rotate, EfParams *ef,
                   cudaStream_t st) {
     k_evals<<<148 * 4, 256, 0, st>>>(node_total, nodes, leaf, rotate, ef);
+    count_launches(1);
 }
 
 }  // namespace rsb

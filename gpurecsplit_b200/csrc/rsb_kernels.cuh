@@ -72,7 +72,13 @@ struct EfParams {
     uint64_t total_bits;       // descriptor bits before the sentinel
     uint64_t desc_words;       // descriptor words incl. the sentinel
     uint64_t evals_alg;
+    uint64_t evals_stage[kNumStages];
 };
+
+// Kernels launched by this library (all threads), for the launch accounting of rsb_stats.
+void count_launches(uint64_t k);
+uint64_t launches_so_far();
+void probe_eval_rate(int num_sms, uint64_t *out_evals, cudaStream_t st);
 void launch_bucket_bits(const uint64_t *node_base, uint64_t nbuckets, NodeArrays nodes, DevTables tab,
                         uint32_t *bits, uint32_t *fixed_bits, DevStatus *status, cudaStream_t st);
 void launch_write_rice(const uint64_t *node_base, uint64_t nbuckets, NodeArrays nodes, DevTables tab,

@@ -106,6 +106,7 @@ void exclusive_scan_u32(const uint32_t *in, uint64_t *out, size_t n, ScanTmp tmp
     k_scan_reduce<<<blocks, kScanThreads, 0, st>>>(in, n, tmp.block_sums);
     k_scan_blocks<<<1, 1024, 0, st>>>(tmp.block_sums, blocks);
     k_scan_final<<<blocks, kScanThreads, 0, st>>>(in, n, tmp.block_sums, out);
+    count_launches(3);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -344,10 +345,12 @@ int grid_for(uint64_t n, int threads, int cap) {
 
 void launch_hash_u64(const uint64_t *keys, uint64_t n, uint64_t *out128, cudaStream_t st) {
     k_hash_u64<<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(keys, n, (ulonglong2 *)out128);
+    count_launches(1);
 }
 
 void launch_hash_strings(const uint8_t *bytes, const uint64_t *offsets, uint64_t n, uint64_t *out128, cudaStream_t st) {
     k_hash_strings<<<grid_for(n, 128, 148 * 32), 128, 0, st>>>(bytes, offsets, n, (ulonglong2 *)out128);
+    count_launches(1);
 }
 
 void launch_bucket_count(const uint64_t *keys128, uint64_t n, uint64_t nb, uint32_t *counts, cudaStream_t st) {
@@ -358,29 +361,35 @@ void launch_bucket_count(const uint64_t *keys128, uint64_t n, uint64_t nb, uint3
     } else {
         k_bucket_count_global<<<grid_for(n, 256, 148 * 16), 256, 0, st>>>((const ulonglong2 *)keys128, n, nb, counts);
     }
+    count_launches(1);
 }
 
 void launch_bucket_check(const uint32_t *counts, uint64_t nb, DevStatus *status, cudaStream_t st) {
     k_bucket_check<<<grid_for(nb, 256, 148 * 8), 256, 0, st>>>(counts, nb, status);
+    count_launches(1);
 }
 
 void launch_bucket_scatter(const uint64_t *keys128, uint64_t n, uint64_t nb, const uint64_t *acc, uint32_t *cursor,
                            uint64_t *sorted, cudaStream_t st) {
     cudaMemsetAsync(cursor, 0, nb * sizeof(uint32_t), st);
     k_bucket_scatter<<<grid_for(n, 256, 148 * 16), 256, 0, st>>>((const ulonglong2 *)keys128, n, nb, acc, cursor, sorted);
+    count_launches(1);
 }
 
 void launch_bucket_sort(uint64_t *sorted, const uint64_t *acc, uint64_t nb, DevStatus *status, cudaStream_t st) {
     k_bucket_sort<<<grid_for(nb, 1, 148 * 6), kSortThreads, 0, st>>>(sorted, acc, nb, status);
+    count_launches(1);
 }
 
 void launch_bucket_nodes(const uint64_t *acc, uint64_t nb, DevTables tab, uint32_t *node_count, cudaStream_t st) {
     k_bucket_nodes<<<grid_for(nb, 256, 148 * 8), 256, 0, st>>>(acc, nb, tab, node_count);
+    count_launches(1);
 }
 
 void launch_tree_emit(const uint64_t *acc, uint64_t nb, const uint64_t *node_base, Shape sh, NodeArrays nodes,
                       cudaStream_t st) {
     k_tree_emit<<<grid_for(nb, 64, 148 * 16), 64, 0, st>>>(acc, nb, node_base, sh, nodes);
+    count_launches(1);
 }
 
 void launch_stage_lists(const uint8_t *stage, const uint64_t *total_nodes, uint32_t max_nodes, uint32_t *stage_info,
@@ -390,6 +399,7 @@ void launch_stage_lists(const uint8_t *stage, const uint64_t *total_nodes, uint3
     k_stage_hist<<<g, 256, 0, st>>>(stage, total_nodes, stage_info);
     k_stage_bases<<<1, 32, 0, st>>>(stage_info);
     k_stage_scatter<<<g, 256, 0, st>>>(stage, total_nodes, stage_info, lists);
+    count_launches(3);
 }
 
 }  // namespace rsb

@@ -540,10 +540,57 @@ void search_higher(const SearchCtx &c, int depth, cudaStream_t st) {
     const size_t smem = kMaxBucketSize * sizeof(uint64_t);
     cudaFuncSetAttribute(k_search_higher, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_search_higher<<<persistent_grid(k_search_higher, smem, c.num_sms), kThreads, smem, st>>>(c, depth);
+    count_launches(1);
 }
 
-void search_aggr(const SearchCtx &c, int stage, cudaStream_t st) { RSB_LEAF_SWITCH(c.sh.leaf, run_aggr, c, stage, st); }
-void partition_aggr(const SearchCtx &c, int stage, cudaStream_t st) { RSB_LEAF_SWITCH(c.sh.leaf, run_partition, c, stage, st); }
-void search_leaves(const SearchCtx &c, int stage, cudaStream_t st) { RSB_LEAF_SWITCH(c.sh.leaf, run_leaves, c, stage, st); }
+void search_aggr(const SearchCtx &c, int stage, cudaStream_t st) {
+    RSB_LEAF_SWITCH(c.sh.leaf, run_aggr, c, stage, st);
+    count_launches(1);
+}
+void partition_aggr(const SearchCtx &c, int stage, cudaStream_t st) {
+    RSB_LEAF_SWITCH(c.sh.leaf, run_partition, c, stage, st);
+    count_launches(1);
+}
+void search_leaves(const SearchCtx &c, int stage, cudaStream_t st) {
+    RSB_LEAF_SWITCH(c.sh.leaf, run_leaves, c, stage, st);
+    count_launches(1);
+}
+
+// ---- eval-rate probe ------------------------------------------------------------------
+// The cheapest complete candidate evaluation of any search (64-bit add, remix32, 16-bit
+// threshold compare, count), laid out like the search kernels (keys broadcast from shared
+// memory, four independent candidates per lane) with no scheduling, no reductions and no
+// early exit: the integer ceiling for remixAndRemap32 evaluations on this device.
+namespace {
+constexpr int kProbeKeys = 128;
+constexpr int kProbeIters = 64;
+__global__ void __launch_bounds__(kThreads) k_probe(unsigned long long *sink) {
+    __shared__ uint64_t sk[kProbeKeys];
+    for (int i = threadIdx.x; i < kProbeKeys; i += kThreads) sk[i] = start_seed(i % 20) * (2 * i + 1);
+    __syncthreads();
+    uint32_t cnt[4] = {0, 0, 0, 0};
+    uint64_t bx = start_seed(17) + blockIdx.x * (uint64_t)kThreads + threadIdx.x;
+    for (int it = 0; it < kProbeIters; ++it) {
+        for (int i = 0; i < kProbeKeys; ++i) {
+            const uint64_t t = sk[i] + bx;
+#pragma unroll
+            for (int s = 0; s < 4; ++s) cnt[s] += hash16(t + 32u * s) < 30001u;
+        }
+        bx += 1ull << 32;
+    }
+    const uint32_t tot = cnt[0] + cnt[1] + cnt[2] + cnt[3];
+    if (tot == 0xFFFFFFFFu) atomicAdd(sink, 1ull);  // keeps the loop alive
+}
+}  // namespace
+
+void probe_eval_rate(int num_sms, uint64_t *out_evals, cudaStream_t st) {
+    const int g = persistent_grid(k_probe, 0, num_sms) * 4;
+    unsigned long long *sink = nullptr;
+    cudaMallocAsync((void **)&sink, 8, st);
+    k_probe<<<g, kThreads, 0, st>>>(sink);
+    cudaFreeAsync(sink, st);
+    count_launches(1);
+    *out_evals = (uint64_t)g * kThreads * kProbeIters * kProbeKeys * 4;
+}
 
 }  // namespace rsb

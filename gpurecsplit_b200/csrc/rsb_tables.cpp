@@ -1,11 +1,18 @@
 // Per-leaf-size constants: tree shape, Golomb-Rice parameters and node counts.
 #include "rsb_tables.h"
 
+#include <atomic>
 #include <cmath>
 #include <map>
 #include <mutex>
 
+#include "rsb_kernels.cuh"
+
 namespace rsb {
+
+static std::atomic<uint64_t> g_launches{0};
+void count_launches(uint64_t k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+uint64_t launches_so_far() { return g_launches.load(std::memory_order_relaxed); }
 
 // AbstractParallelRecSplit.hpp:106 — Rice parameters of bijection leaves.
 static const uint8_t kBijMemo[25] = {0, 0, 0, 1, 3, 4, 5, 7, 8, 10, 11, 12, 14, 15, 16, 18, 19, 21, 22, 23, 25, 26, 28, 29, 30};

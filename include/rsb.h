@@ -67,6 +67,8 @@ typedef struct rsb_stats {
     double ms_partition;           /* hashing, bucket histogram/scan/scatter, per-bucket sort */
     double ms_search[21];          /* per search stage */
     double ms_encode;              /* Rice + Elias-Fano */
+    uint64_t evals_stage[21];      /* evals_alg split by search stage */
+    uint64_t kernel_launches;      /* kernels this build launched */
 } rsb_stats;
 
 /* ---- engine ------------------------------------------------------------------------ */
@@ -129,6 +131,11 @@ rsb_status rsb_free(rsb_mphf *mphf);
 rsb_status rsb_hash_strings(rsb_engine *engine, const uint8_t *bytes, const uint64_t *offsets, uint64_t n,
                             uint32_t flags, rsb_hash128 *out);
 rsb_status rsb_hash_u64(rsb_engine *engine, const uint64_t *keys, uint64_t n, uint32_t flags, rsb_hash128 *out);
+
+/* Measures the device's rate of remixAndRemap32 candidate evaluations (the primitive of
+ * every seed search) with a synthetic kernel at full occupancy: the integer ceiling the
+ * search kernels are compared with. No reference counterpart. */
+rsb_status rsb_probe_eval_rate(rsb_engine *engine, double *evals_per_second, double *ms);
 
 /* Golomb-Rice table of the engine for one leaf size (3000 entries), the table generated by
  * fill_golomb_rice<LEAF_SIZE>() (AbstractParallelRecSplit.hpp:191-227) and shipped as

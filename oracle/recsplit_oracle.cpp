@@ -389,7 +389,9 @@ struct DoubleEF {
     void build(const std::vector<uint64_t> &cum_keys, const std::vector<uint64_t> &position) {
         num_buckets = cum_keys.size() - 1;
         // :144 — the one floating-point operation of the path (IEEE double, round to nearest).
-        bits_per_key_fixed_point = (uint64_t)((double)(uint64_t(1) << 20) * (position[num_buckets] / (double)cum_keys[num_buckets]));
+        // With no keys this is 0/0; the reference's x86-64 build converts that NaN to 0x8000000000000000.
+        bits_per_key_fixed_point = cum_keys[num_buckets] == 0 ? (uint64_t(1) << 63)
+            : (uint64_t)((double)(uint64_t(1) << 20) * (position[num_buckets] / (double)cum_keys[num_buckets]));
         min_diff = INT64_MAX / 2;
         cum_keys_min_delta = INT64_MAX / 2;
         int64_t prev_bucket_bits = 0;
