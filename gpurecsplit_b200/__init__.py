@@ -98,6 +98,7 @@ def lib():
             "rsb_version": ([], ctypes.c_char_p),
             "rsb_golomb_memo": ([u32, vp], i32),
             "rsb_probe_eval_rate": ([vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)], i32),
+            "rsb_hash_strings_static": ([vp, vp, u64, vp, vp], i32),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -330,6 +331,25 @@ def hash_strings(keys, engine: Optional[Engine] = None) -> np.ndarray:
     n = offsets.size - 1
     out = np.zeros((n, 2), dtype=np.uint64)
     _check(lib().rsb_hash_strings(eng.handle, _ptr(data), _ptr(offsets), n, 0, _ptr(out)), "hash_strings")
+    return out
+
+
+def hash_strings_static(keys, stream: Optional[int] = None) -> np.ndarray:
+    """Device SpookyHash V2 of string keys without any device allocation (rsb_hash_strings_static).
+
+    For callers that cannot allocate device memory; at most 32,768 keys and 1 MiB of key
+    bytes per call. Runs on the current CUDA device.
+    """
+    if isinstance(keys, tuple) and len(keys) == 2 and isinstance(keys[0], np.ndarray):
+        data, offsets = keys
+    else:
+        data, offsets = _strings_to_arrays(keys)
+    data = np.ascontiguousarray(data, dtype=np.uint8)
+    offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+    n = offsets.size - 1
+    out = np.zeros((n, 2), dtype=np.uint64)
+    _check(lib().rsb_hash_strings_static(_ptr(data), _ptr(offsets), n, _ptr(out), ctypes.c_void_p(stream or 0)),
+           "hash_strings_static")
     return out
 
 

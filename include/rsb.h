@@ -132,6 +132,21 @@ rsb_status rsb_hash_strings(rsb_engine *engine, const uint8_t *bytes, const uint
                             uint32_t flags, rsb_hash128 *out);
 rsb_status rsb_hash_u64(rsb_engine *engine, const uint64_t *keys, uint64_t n, uint32_t flags, rsb_hash128 *out);
 
+/* rsb_hash_strings without any device allocation. No counterpart in the reference.
+ * For callers that cannot allocate device memory (a plugin inside a host process that owns
+ * all device memory through its own pool, or a serving thread that must not call cudaMalloc
+ * because it can synchronise the device). Keys i is bytes[offsets[i] .. offsets[i+1]);
+ * bytes, offsets and out are host memory; the work runs on the current device and on
+ * `stream` (a cudaStream_t, NULL for the default stream) and is complete on return. The
+ * results equal rsb_hash_strings'. Staging uses one fixed array of device memory inside the
+ * library (about 1.8 MiB, held by every GPU that loads the library until exit), so at most
+ * 32,768 keys and 1 MiB of key bytes per call: larger inputs return RSB_ERR_BAD_ARG. The
+ * first call on a device resolves that array's address (cudaGetSymbolAddress); make it
+ * before any stream capture. Calls share the array; a process-wide lock held until the
+ * stream finishes keeps their GPU work from overlapping. */
+rsb_status rsb_hash_strings_static(const uint8_t *bytes, const uint64_t *offsets, uint64_t n, rsb_hash128 *out,
+                                   void *stream);
+
 /* Measures the device's rate of remixAndRemap32 candidate evaluations (the primitive of
  * every seed search) with a synthetic kernel at full occupancy: the integer ceiling the
  * search kernels are compared with. No reference counterpart. */
