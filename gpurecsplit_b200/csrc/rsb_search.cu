@@ -164,7 +164,19 @@ __global__ void __launch_bounds__(kThreads) k_search_higher(SearchCtx c, int dep
 // holds at most fanout * SPLIT keys, so a byte can only carry into the next one on
 // candidates that already fail — packed equality is exact equality.
 // ---------------------------------------------------------------------------------------
+//
+// Two-phase evaluation. A seed can only split a node exactly if the keys falling below the
+// part boundary j*SPLIT closest to m/2 number exactly j*SPLIT — a necessary condition that
+// costs one threshold compare per key (hash16 < ceil(j*SPLIT*2^16/m)) instead of a part
+// count. Phase A applies it to every seed of a window (4 per lane); the few survivors
+// (about 1/sqrt(2*pi*m*p*(1-p)) of them, 3-8 %) go to a per-warp queue in shared memory,
+// and phase B gives each lane one queued seed for the exact part count. A warp drains its
+// queue before it leaves a node, so every seed below the node's final best is still fully
+// checked and the minimum is unchanged.
+// ---------------------------------------------------------------------------------------
 constexpr int kAggrSeedsPerLane = 4;
+constexpr uint32_t kAggrWindow = 32 * kAggrSeedsPerLane;
+constexpr int kQueueCap = 32 + (int)kAggrWindow;  // < 32 pending after a drain + one window
 
 template <int LEAF, int STAGE>
 struct AggrCfg {
@@ -173,50 +185,82 @@ struct AggrCfg {
     static constexpr uint32_t MAXF = (MAXM + SPLIT - 1) / SPLIT;
     static constexpr bool WIDE = MAXF > 4;
     static constexpr uint64_t SEED_INDEX = STAGE == kStageUpper ? 17 : 18;
+    static constexpr uint32_t WARP_WORDS = MAXM + kQueueCap;  // keys + candidate queue
 };
 
-template <int LEAF, int STAGE, bool FULL, bool WIDE>
-__device__ __forceinline__ uint32_t aggr_window(const uint64_t *sk, uint32_t m, uint32_t fan, uint64_t bx,
-                                                uint32_t tlo, uint32_t thi) {
+__device__ __forceinline__ uint64_t warp_min_u64(uint64_t v) {
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        const uint64_t o = __shfl_xor_sync(0xffffffffu, v, d);
+        v = o < v ? o : v;
+    }
+    return v;
+}
+
+// Exact (packed) part counts of one candidate seed sx over the node's keys.
+template <int LEAF, int STAGE, bool WIDE>
+__device__ __forceinline__ bool aggr_exact(const uint64_t *sk, uint32_t m, uint32_t fan, bool full, uint64_t sx,
+                                           uint32_t tlo, uint32_t thi) {
     using C = AggrCfg<LEAF, STAGE>;
-    constexpr int S = kAggrSeedsPerLane;
-    uint32_t lo[S], hi[S];
-#pragma unroll
-    for (int s = 0; s < S; ++s) lo[s] = hi[s] = 0;
-    for (uint32_t i = 0; i < m; ++i) {
-        const uint64_t t = sk[i] + bx;
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            const uint32_t h = hash16(t + 32u * s);
-            const uint32_t p = FULL ? (h * fan) >> 16 : ((h * m) >> 16) / C::SPLIT;
+    uint32_t lo = 0, hi = 0;
+    if (full) {
+        for (uint32_t i = 0; i < m; ++i) {
+            const uint32_t p = (hash16(sk[i] + sx) * fan) >> 16;
             if (WIDE) {
-                lo[s] += shl_clamp(1u, 8 * p);
-                hi[s] += shl_clamp(1u, 8 * p - 32);
+                lo += shl_clamp(1u, 8 * p);
+                hi += shl_clamp(1u, 8 * p - 32);
             } else {
-                lo[s] += 1u << (8 * p);
+                lo += 1u << (8 * p);
+            }
+        }
+    } else {
+        for (uint32_t i = 0; i < m; ++i) {
+            const uint32_t p = ((hash16(sk[i] + sx) * m) >> 16) / C::SPLIT;
+            if (WIDE) {
+                lo += shl_clamp(1u, 8 * p);
+                hi += shl_clamp(1u, 8 * p - 32);
+            } else {
+                lo += 1u << (8 * p);
             }
         }
     }
-    uint32_t best = 0xFFFFFFFFu;
-#pragma unroll
-    for (int s = S - 1; s >= 0; --s)
-        if (lo[s] == tlo && (!WIDE || hi[s] == thi)) best = (threadIdx.x & 31) + 32u * s;
-    return best;
+    return lo == tlo && (!WIDE || hi == thi);
+}
+
+// Phase B: checks the last `take` (<= 32) queued candidates, one per lane, and merges the
+// smallest success into the node's seed. Candidates not below `best` cannot lower it.
+template <int LEAF, int STAGE>
+__device__ __forceinline__ void aggr_drain(const uint64_t *sk, uint64_t *q, uint32_t &qn, uint32_t take, uint32_t m,
+                                           uint32_t fan, bool full, uint64_t seed, uint32_t tlo, uint32_t thi,
+                                           uint64_t best, uint64_t *node_seed) {
+    using C = AggrCfg<LEAF, STAGE>;
+    const int lane = threadIdx.x & 31;
+    const bool active = lane < (int)take;
+    const uint64_t x = active ? q[qn - take + lane] : ~0ull;
+    __syncwarp();
+    bool ok = false;
+    if (active && x < best) ok = aggr_exact<LEAF, STAGE, C::WIDE>(sk, m, fan, full, seed + x, tlo, thi);
+    const uint64_t v = warp_min_u64(ok ? x : ~0ull);
+    if (lane == 0 && v != ~0ull) atomicMin((unsigned long long *)node_seed, (unsigned long long)v);
+    qn -= take;
 }
 
 template <int LEAF, int STAGE>
 __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
     using C = AggrCfg<LEAF, STAGE>;
-    constexpr uint32_t W = 32 * kAggrSeedsPerLane;
+    constexpr int S = kAggrSeedsPerLane;
+    constexpr uint32_t W = kAggrWindow;
     extern __shared__ uint64_t smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint64_t *sk = smem + warp * C::MAXM;
+    uint64_t *sk = smem + warp * C::WARP_WORDS;
+    uint64_t *q = sk + C::MAXM;
+    const unsigned below = (1u << lane) - 1;
     const uint32_t gw = blockIdx.x * kWarpsPerCta + warp;
     const uint32_t count = c.stage_info[STAGE];
     const uint32_t base = c.stage_info[kNumStages + STAGE];
     const uint64_t seed = start_seed(C::SEED_INDEX);
     uint32_t rng = gw * 2654435761u + 12345u;
-    uint32_t node = kEmpty, m = 0, fan = 0, tlo = 0, thi = 0;
+    uint32_t node = kEmpty, m = 0, fan = 0, tlo = 0, thi = 0, thr = 0, cstar = 0, qn = 0;
     bool owner = false, full = false;
     uint64_t budget = 0;
     for (;;) {
@@ -248,31 +292,54 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
                 if (j < 4) tlo |= t << (8 * j);
                 else thi |= t << (8 * (j - 4));
             }
+            // filter boundary: the part boundary j*SPLIT (1 <= j < fan) closest to m/2
+            uint32_t js = 1;
+            for (uint32_t j = 2; j < fan; ++j) {
+                const int dj = (int)(2 * j * C::SPLIT) - (int)m, db = (int)(2 * js * C::SPLIT) - (int)m;
+                if (abs(dj) < abs(db)) js = j;
+            }
+            cstar = js * C::SPLIT;
+            thr = (uint32_t)((((uint64_t)cstar << 16) + m - 1) / m);
             budget = budget_for(c, m);
+            qn = 0;
         }
         uint32_t w = 0;
         if (lane == 0) w = atomicAdd(&c.nodes.next_win[node], 1u);
         w = __shfl_sync(0xffffffffu, w, 0);
         const uint64_t x0 = (uint64_t)w * W;
-        const uint64_t best = vload64(&c.nodes.seed[node]);
+        uint64_t best = vload64(&c.nodes.seed[node]);
         if (x0 >= best || x0 >= budget) {
+            while (qn > 0) {
+                best = vload64(&c.nodes.seed[node]);
+                aggr_drain<LEAF, STAGE>(sk, q, qn, min(qn, 32u), m, fan, full, seed, tlo, thi, best, &c.nodes.seed[node]);
+            }
             if (x0 < best && lane == 0) atomicMin((unsigned long long *)&c.nodes.seed[node], (unsigned long long)kSeedFailed);
             if (owner && lane == 0) c.slots[gw] = kEmpty;
             node = kEmpty;
             continue;
         }
+        // phase A: threshold count for S seeds per lane
         const uint64_t bx = seed + x0 + lane;
-        uint32_t off;
-        if (C::WIDE) {
-            off = full ? aggr_window<LEAF, STAGE, true, C::WIDE>(sk, m, fan, bx, tlo, thi)
-                       : aggr_window<LEAF, STAGE, false, C::WIDE>(sk, m, fan, bx, tlo, thi);
-        } else {
-            off = full ? aggr_window<LEAF, STAGE, true, false>(sk, m, fan, bx, tlo, thi)
-                       : aggr_window<LEAF, STAGE, false, false>(sk, m, fan, bx, tlo, thi);
+        uint32_t cnt[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) cnt[s] = 0;
+        for (uint32_t i = 0; i < m; ++i) {
+            const uint64_t t = sk[i] + bx;
+#pragma unroll
+            for (int s = 0; s < S; ++s) cnt[s] += hash16(t + 32u * s) < thr;
         }
-        off = __reduce_min_sync(0xffffffffu, off);
-        if (off != 0xFFFFFFFFu && lane == 0)
-            atomicMin((unsigned long long *)&c.nodes.seed[node], (unsigned long long)(x0 + off));
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const bool pass = cnt[s] == cstar;
+            const unsigned b = __ballot_sync(0xffffffffu, pass);
+            if (pass) q[qn + __popc(b & below)] = x0 + lane + 32u * s;
+            qn += __popc(b);
+        }
+        __syncwarp();
+        while (qn >= 32) {
+            best = vload64(&c.nodes.seed[node]);
+            aggr_drain<LEAF, STAGE>(sk, q, qn, 32u, m, fan, full, seed, tlo, thi, best, &c.nodes.seed[node]);
+        }
     }
 }
 
@@ -327,15 +394,49 @@ __global__ void __launch_bounds__(kThreads) k_partition_aggr(SearchCtx c) {
 // ---------------------------------------------------------------------------------------
 // Leaves. Rotation leaves (m == LEAF): left = even `second`, right = odd; for base b the
 // encoded seed is b*LEAF + r with r the least left rotation of the right mask that fills
-// the complement of the left mask. Brute-force leaves: the first x whose m bit positions
-// are all distinct.
+// the complement of the left mask. A base can only succeed if the left keys land on
+// distinct bits, so phase A computes the left mask of every base and queues (base, mask)
+// for the few collision-free ones; phase B computes their right masks and rotations.
+// Brute-force leaves: the first x whose m bit positions are all distinct.
 // ---------------------------------------------------------------------------------------
 constexpr int kLeafSeedsPerLane = 4;
+constexpr int kLeafQueueCap = 32 + 32 * kLeafSeedsPerLane;
 
 template <int LEAF>
 __device__ __forceinline__ uint32_t rotl_leaf(uint32_t v, uint32_t r) {
     constexpr uint32_t full = (LEAF == 32) ? 0xFFFFFFFFu : ((1u << LEAF) - 1);
     return ((v << r) | (v >> (LEAF - r))) & full;
+}
+
+// Phase B of rotation leaves: each lane takes one queued (base, left mask).
+template <int LEAF>
+__device__ __forceinline__ void leaf_drain(const uint64_t *sk, uint32_t nl, const uint64_t *qb, const uint32_t *qm,
+                                           uint32_t &qn, uint32_t take, uint64_t seed, uint64_t best,
+                                           uint64_t *node_seed) {
+    constexpr uint32_t full = (1u << LEAF) - 1;
+    const int lane = threadIdx.x & 31;
+    const bool active = lane < (int)take;
+    const uint64_t b = active ? qb[qn - take + lane] : 0;
+    const uint32_t ml = active ? qm[qn - take + lane] : 0;
+    __syncwarp();
+    uint64_t enc = ~0ull;
+    if (active && b * LEAF < best) {
+        const uint64_t bx = seed + b * LEAF;
+        uint32_t mr = 0;
+        for (uint32_t i = nl; i < (uint32_t)LEAF; ++i) mr |= 1u << remap16(sk[i] + bx, LEAF);
+        if (__popc(mr) == LEAF - (int)nl) {
+            const uint32_t want = full & ~ml;
+            for (uint32_t r = 0; r < (uint32_t)LEAF; ++r) {
+                if (rotl_leaf<LEAF>(mr, r) == want) {
+                    enc = b * LEAF + r;
+                    break;
+                }
+            }
+        }
+    }
+    enc = warp_min_u64(enc);
+    if (lane == 0 && enc != ~0ull) atomicMin((unsigned long long *)node_seed, (unsigned long long)enc);
+    qn -= take;
 }
 
 template <int LEAF, bool ROT>
@@ -344,8 +445,13 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
     constexpr int S = kLeafSeedsPerLane;
     constexpr uint32_t W = 32 * S;
     __shared__ uint64_t skeys[kWarpsPerCta][LEAF];
+    __shared__ uint64_t s_qb[ROT ? kWarpsPerCta : 1][ROT ? kLeafQueueCap : 1];
+    __shared__ uint32_t s_qm[ROT ? kWarpsPerCta : 1][ROT ? kLeafQueueCap : 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint64_t *sk = skeys[warp];
+    uint64_t *qb = s_qb[ROT ? warp : 0];
+    uint32_t *qm = s_qm[ROT ? warp : 0];
+    uint32_t qn = 0;
     const uint32_t gw = blockIdx.x * kWarpsPerCta + warp;
     const uint32_t count = c.stage_info[STAGE];
     const uint32_t base = c.stage_info[kNumStages + STAGE];
@@ -385,14 +491,21 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
             }
             __syncwarp();
             budget = budget_for(c, m);
+            qn = 0;
         }
         uint32_t w = 0;
         if (lane == 0) w = atomicAdd(&c.nodes.next_win[node], 1u);
         w = __shfl_sync(0xffffffffu, w, 0);
         const uint64_t x0 = (uint64_t)w * W;                   // first base (ROT) or seed of the window
         const uint64_t enc0 = ROT ? x0 * LEAF : x0;            // first encoded seed of the window
-        const uint64_t best = vload64(&c.nodes.seed[node]);
+        uint64_t best = vload64(&c.nodes.seed[node]);
         if (enc0 >= best || enc0 >= budget) {
+            if (ROT) {
+                while (qn > 0) {
+                    best = vload64(&c.nodes.seed[node]);
+                    leaf_drain<LEAF>(sk, nl, qb, qm, qn, min(qn, 32u), seed, best, &c.nodes.seed[node]);
+                }
+            }
             if (enc0 < best && lane == 0) atomicMin((unsigned long long *)&c.nodes.seed[node], (unsigned long long)kSeedFailed);
             if (owner && lane == 0) c.slots[gw] = kEmpty;
             node = kEmpty;
@@ -400,24 +513,28 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
         }
         uint32_t off = 0xFFFFFFFFu;
         if (ROT) {
-            constexpr uint32_t full = (1u << LEAF) - 1;
+            // phase A: left masks of S bases per lane; queue the collision-free ones
+            const unsigned below = (1u << lane) - 1;
 #pragma unroll
-            for (int s = S - 1; s >= 0; --s) {
+            for (int s = 0; s < S; ++s) {
                 const uint64_t b = x0 + lane + 32u * s;
                 const uint64_t bx = seed + b * LEAF;
-                uint32_t ml = 0, mr = 0;
+                uint32_t ml = 0;
                 for (uint32_t i = 0; i < nl; ++i) ml |= 1u << remap16(sk[i] + bx, LEAF);
-                for (uint32_t i = nl; i < (uint32_t)LEAF; ++i) mr |= 1u << remap16(sk[i] + bx, LEAF);
-                if (__popc(ml) == (int)nl && __popc(mr) == LEAF - (int)nl) {
-                    const uint32_t want = full & ~ml;
-                    for (uint32_t r = 0; r < (uint32_t)LEAF; ++r) {
-                        if (rotl_leaf<LEAF>(mr, r) == want) {
-                            off = (lane + 32u * s) * LEAF + r;
-                            break;
-                        }
-                    }
+                const bool pass = __popc(ml) == (int)nl;
+                const unsigned bal = __ballot_sync(0xffffffffu, pass);
+                if (pass) {
+                    qb[qn + __popc(bal & below)] = b;
+                    qm[qn + __popc(bal & below)] = ml;
                 }
+                qn += __popc(bal);
             }
+            __syncwarp();
+            while (qn >= 32) {
+                best = vload64(&c.nodes.seed[node]);
+                leaf_drain<LEAF>(sk, nl, qb, qm, qn, 32u, seed, best, &c.nodes.seed[node]);
+            }
+            continue;
         } else {
             const uint32_t full = (1u << m) - 1;
 #pragma unroll
@@ -448,7 +565,7 @@ template <int LEAF>
 void run_aggr(const SearchCtx &c, int stage, cudaStream_t st) {
     if (stage == kStageUpper) {
         using C = AggrCfg<LEAF, kStageUpper>;
-        const size_t smem = kWarpsPerCta * C::MAXM * sizeof(uint64_t);
+        const size_t smem = kWarpsPerCta * C::WARP_WORDS * sizeof(uint64_t);
         auto k = k_search_aggr<LEAF, kStageUpper>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         int g = persistent_grid(k, smem, c.num_sms);
@@ -458,7 +575,7 @@ void run_aggr(const SearchCtx &c, int stage, cudaStream_t st) {
         k<<<g, kThreads, smem, st>>>(cc);
     } else {
         using C = AggrCfg<LEAF, kStageLower>;
-        const size_t smem = kWarpsPerCta * C::MAXM * sizeof(uint64_t);
+        const size_t smem = kWarpsPerCta * C::WARP_WORDS * sizeof(uint64_t);
         auto k = k_search_aggr<LEAF, kStageLower>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         int g = persistent_grid(k, smem, c.num_sms);

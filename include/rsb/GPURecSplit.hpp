@@ -176,7 +176,9 @@ class GPURecSplit {
         };
         auto take_vec = [&]() {
             uint64_t n;
-            std::memcpy(&n, buf.data() + take(8), 8);
+            const size_t at = take(8);  // take() may reallocate buf: read the count after it
+            std::memcpy(&n, buf.data() + at, 8);
+            if (n > (uint64_t(1) << 40)) throw std::runtime_error("GPURecSplit: malformed stream");
             take(n * 8);
         };
         take(24);
