@@ -20,7 +20,8 @@ from typing import Iterable, Optional, Sequence, Union
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "_lib", "librsb.so")
+# RSB_LIBRARY selects another build of librsb.so (e.g. one compiled with different flags).
+LIB_PATH = os.environ.get("RSB_LIBRARY") or os.path.join(_HERE, "_lib", "librsb.so")
 
 RSB_ROTATE = 1
 RSB_KEYS_ON_DEVICE = 2

@@ -10,7 +10,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
-#include "../../include/rsb.h"
+#include "rsb.h"  // include/ is on the include path of every build
 
 namespace rsb {
 

@@ -53,6 +53,40 @@ __device__ __forceinline__ uint32_t shl_clamp(uint32_t a, uint32_t b) {
 // Low 16 bits of remix32(hi ^ lo) of a 64-bit candidate.
 __device__ __forceinline__ uint32_t hash16(uint64_t v) { return remix32(uint32_t(v >> 32) ^ uint32_t(v)) & 0xFFFFu; }
 
+// cnt[s] += #{keys k : hash16(k + bu + lane + 32 s) < thr} for s < S, where bu is the
+// warp-uniform window base. The 64-bit key + base sum is formed once per key; when its low
+// word cannot carry into the high word within the window (all but ~S*32 / 2^32 of the
+// keys), every candidate differs only in the low word, so the high word's share of
+// remix32's first xor-shift (H = hi ^ hi >> 16) is hoisted and each candidate costs a
+// 32-bit add. The compare is done on h16 << 16 = (z << 16) ^ (z & 0xFFFF0000).
+template <int S>
+__device__ __forceinline__ void threshold_counts(const uint64_t *sk, uint32_t m, uint64_t bu, uint32_t thr,
+                                                 uint32_t *cnt) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t thr16 = thr << 16;
+#pragma unroll 4
+    for (uint32_t i = 0; i < m; ++i) {
+        const uint64_t tu = sk[i] + bu;
+        const uint32_t lo0 = (uint32_t)tu, hi = (uint32_t)(tu >> 32);
+        if (lo0 > 0xFFFFFFFFu - 32u * S) {
+#pragma unroll
+            for (int s = 0; s < S; ++s) cnt[s] += hash16(tu + lane + 32u * s) < thr;
+        } else {
+            const uint32_t H = hi ^ (hi >> 16);
+            const uint32_t l0 = lo0 + lane;
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const uint32_t lo = l0 + 32u * s;
+                uint32_t z = lo ^ (lo >> 16) ^ H;
+                z *= 0x85ebca6bu;
+                z ^= z >> 13;
+                z *= 0xc2b2ae35u;
+                cnt[s] += ((z << 16) ^ (z & 0xFFFF0000u)) < thr16;
+            }
+        }
+    }
+}
+
 __device__ __forceinline__ uint64_t budget_for(const SearchCtx &c, uint32_t m) {
     const uint32_t g = c.tab.memo[m] >> 27;
     const uint32_t sh = min(g + c.budget_shift, 62u);
@@ -174,7 +208,7 @@ __global__ void __launch_bounds__(kThreads) k_search_higher(SearchCtx c, int dep
 // queue before it leaves a node, so every seed below the node's final best is still fully
 // checked and the minimum is unchanged.
 // ---------------------------------------------------------------------------------------
-constexpr int kAggrSeedsPerLane = 4;
+constexpr int kAggrSeedsPerLane = 8;
 constexpr uint32_t kAggrWindow = 32 * kAggrSeedsPerLane;
 constexpr int kQueueCap = 32 + (int)kAggrWindow;  // < 32 pending after a drain + one window
 
@@ -318,16 +352,11 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
             node = kEmpty;
             continue;
         }
-        // phase A: threshold count for S seeds per lane
-        const uint64_t bx = seed + x0 + lane;
+        // phase A: threshold count for S seeds per lane (seeds x0 + lane + 32 s)
         uint32_t cnt[S];
 #pragma unroll
         for (int s = 0; s < S; ++s) cnt[s] = 0;
-        for (uint32_t i = 0; i < m; ++i) {
-            const uint64_t t = sk[i] + bx;
-#pragma unroll
-            for (int s = 0; s < S; ++s) cnt[s] += hash16(t + 32u * s) < thr;
-        }
+        threshold_counts<S>(sk, m, seed + x0, thr, cnt);
 #pragma unroll
         for (int s = 0; s < S; ++s) {
             const bool pass = cnt[s] == cstar;
@@ -406,6 +435,33 @@ template <int LEAF>
 __device__ __forceinline__ uint32_t rotl_leaf(uint32_t v, uint32_t r) {
     constexpr uint32_t full = (LEAF == 32) ? 0xFFFFFFFFu : ((1u << LEAF) - 1);
     return ((v << r) | (v >> (LEAF - r))) & full;
+}
+
+// Left masks of the S bases x0 + lane + 32 s of a rotation-leaf window (bu = SEED + x0*LEAF),
+// with the same hoisting of the key + base sum as threshold_counts.
+template <int LEAF, int S>
+__device__ __forceinline__ void left_masks(const uint64_t *sk, uint32_t nl, uint64_t bu, uint32_t *ml) {
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint32_t i = 0; i < nl; ++i) {
+        const uint64_t tu = sk[i] + bu;
+        const uint32_t lo0 = (uint32_t)tu, hi = (uint32_t)(tu >> 32);
+        if (lo0 > 0xFFFFFFFFu - 32u * S * LEAF) {
+#pragma unroll
+            for (int s = 0; s < S; ++s) ml[s] |= 1u << remap16(tu + (lane + 32u * s) * LEAF, LEAF);
+        } else {
+            const uint32_t H = hi ^ (hi >> 16);
+            const uint32_t l0 = lo0 + lane * LEAF;
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const uint32_t lo = l0 + 32u * s * LEAF;
+                uint32_t z = lo ^ (lo >> 16) ^ H;
+                z *= 0x85ebca6bu;
+                z ^= z >> 13;
+                z *= 0xc2b2ae35u;
+                ml[s] |= 1u << ((((z ^ (z >> 16)) & 0xFFFFu) * LEAF) >> 16);
+            }
+        }
+    }
 }
 
 // Phase B of rotation leaves: each lane takes one queued (base, left mask).
@@ -515,17 +571,18 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
         if (ROT) {
             // phase A: left masks of S bases per lane; queue the collision-free ones
             const unsigned below = (1u << lane) - 1;
+            uint32_t ml[S];
+#pragma unroll
+            for (int s = 0; s < S; ++s) ml[s] = 0;
+            left_masks<LEAF, S>(sk, nl, seed + x0 * LEAF, ml);
 #pragma unroll
             for (int s = 0; s < S; ++s) {
                 const uint64_t b = x0 + lane + 32u * s;
-                const uint64_t bx = seed + b * LEAF;
-                uint32_t ml = 0;
-                for (uint32_t i = 0; i < nl; ++i) ml |= 1u << remap16(sk[i] + bx, LEAF);
-                const bool pass = __popc(ml) == (int)nl;
+                const bool pass = __popc(ml[s]) == (int)nl;
                 const unsigned bal = __ballot_sync(0xffffffffu, pass);
                 if (pass) {
                     qb[qn + __popc(bal & below)] = b;
-                    qm[qn + __popc(bal & below)] = ml;
+                    qm[qn + __popc(bal & below)] = ml[s];
                 }
                 qn += __popc(bal);
             }
