@@ -315,6 +315,81 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------------------
+# Batched form: many independent key sets in one pipeline vs back-to-back plain builds
+# ---------------------------------------------------------------------------------------
+def batch_workload(nsets: int, seed0: int = 1000):
+    """Set i: round(exp(U[ln 1e3, ln 1e6])) u64 keys from splitmix64 seeded seed0 + i."""
+    rng = np.random.default_rng(7)
+    sizes = np.rint(np.exp(rng.uniform(np.log(1e3), np.log(1e6), nsets))).astype(np.int64)
+    offsets = np.zeros(nsets + 1, dtype=np.uint64)
+    offsets[1:] = np.cumsum(sizes)
+    keys = np.empty(int(offsets[-1]), dtype=np.uint64)
+    for i in range(nsets):
+        keys[offsets[i]:offsets[i + 1]] = splitmix64_keys(seed0 + i, int(sizes[i]))
+    return keys, offsets
+
+
+def run_batch(args) -> None:
+    import torch
+    import gpurecsplit_b200 as rsb
+
+    leaf, b = 12, 1000
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    engine = rsb.Engine(0, stream.cuda_stream)
+    keys, offsets = batch_workload(args.sets)
+    n = int(offsets[-1])
+    keys_dev = torch.from_numpy(keys.view(np.int64)).to("cuda")
+    torch.cuda.synchronize()
+    base = keys_dev.data_ptr()
+
+    def batched():
+        funcs, st = rsb.build_batch(base, offsets, b, leaf, key_type="u64", engine=engine, keys_on_device=True)
+        return funcs, st
+
+    def plain_all():
+        out = []
+        for i in range(args.sets):
+            lo, hi = int(offsets[i]), int(offsets[i + 1])
+            out.append(rsb.GPURecSplit.from_device(base + 8 * lo, hi - lo, b, leaf, key_type="u64", engine=engine,
+                                                   device_only=False))
+        return out
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        r = fn()
+        e.record(stream)
+        e.synchronize()
+        return r, s.elapsed_time(e)
+
+    batched()  # warm-up (sizes the engine's scratch)
+    plain_all()
+    with ClockSampler(0) as clocks:
+        (funcs, st), t_batch = timed(batched)
+        plain, t_plain = timed(plain_all)
+    same = all(f.serialize() == p.serialize() for f, p in zip(funcs, plain))
+    line = {
+        "metric": "batched keys/s (log-uniform sets in [1e3,1e6], l=12, b=1000)", "value": n / (t_batch * 1e-3),
+        "unit": "keys/s", "higher_is_better": True, "n_gpus": 1, "steps": 1, "warmup": 1,
+        "ms_per_step": t_batch, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": f"{args.sets} key sets, sizes round(exp(U[ln 1e3, ln 1e6])) (numpy seed 7), "
+                               f"set i = splitmix64(seed 1000+i) u64 keys, l={leaf}, b={b}, rotation",
+                   "sets": args.sets, "keys": n},
+        "plain_back_to_back": {"keys_per_s": n / (t_plain * 1e-3), "ms": t_plain},
+        "speedup_vs_plain": t_plain / t_batch,
+        "identical_to_plain": same,
+        "stage_ms": {"partition": st["ms_partition"], "search": {str(i): round(v, 3) for i, v in
+                                                                 enumerate(st["ms_search"]) if v > 0},
+                     "encode": st["ms_encode"], "total": st["ms_total"]},
+        "gpu_launches": st["kernel_launches"], "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    engine.close()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -325,7 +400,12 @@ def main() -> None:
     ap.add_argument("--cpu-buckets", type=int, default=48)
     ap.add_argument("--ref-buckets", type=int, default=24)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", default="plain", choices=["plain", "batch"])
+    ap.add_argument("--sets", type=int, default=1000)
     args = ap.parse_args()
+    if args.mode == "batch":
+        run_batch(args)
+        return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))

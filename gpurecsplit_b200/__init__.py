@@ -100,6 +100,8 @@ def lib():
             "rsb_golomb_memo": ([u32, vp], i32),
             "rsb_probe_eval_rate": ([vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)], i32),
             "rsb_hash_strings_static": ([vp, vp, u64, vp, vp], i32),
+            "rsb_build_batch_hash128": ([vp, vp, vp, u32, u64, u32, u32, vp, ctypes.POINTER(Stats)], i32),
+            "rsb_build_batch_u64": ([vp, vp, vp, u32, u64, u32, u32, vp, ctypes.POINTER(Stats)], i32),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -318,6 +320,45 @@ class GPURecSplit:
             self.close()
         except Exception:
             pass
+
+
+def build_batch(keys: np.ndarray, set_offsets, bucket_size: int, leaf_size: int, rotate: bool = True,
+                key_type: Optional[str] = None, engine: Optional[Engine] = None, keys_on_device: bool = False,
+                n_keys: Optional[int] = None):
+    """Builds one function per key set in a single device pipeline (rsb_build_batch_*).
+
+    Set s is keys[set_offsets[s]:set_offsets[s+1]]. ``keys`` is a (n, 2) uint64 hash128 array
+    or (``key_type="u64"``) a uint64 array, or with ``keys_on_device`` a device pointer (int).
+    Returns (list of GPURecSplit, stats dict); each function equals the plain build of its set.
+    """
+    eng = engine or default_engine()
+    offsets = np.ascontiguousarray(set_offsets, dtype=np.uint64)
+    nsets = offsets.size - 1
+    outs = (ctypes.c_void_p * max(nsets, 1))()
+    stats = Stats()
+    flags = (RSB_ROTATE if rotate else 0) | (RSB_KEYS_ON_DEVICE if keys_on_device else 0)
+    L = lib()
+    if keys_on_device:
+        kp = ctypes.c_void_p(keys)
+        if key_type is None:
+            key_type = "hash128"
+    else:
+        if key_type is None:
+            key_type = "hash128" if keys.ndim == 2 else "u64"
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        kp = _ptr(keys)
+    if key_type == "hash128":
+        st = L.rsb_build_batch_hash128(eng.handle, kp, _ptr(offsets), nsets, bucket_size, leaf_size, flags, outs,
+                                       ctypes.byref(stats))
+    elif key_type == "u64":
+        st = L.rsb_build_batch_u64(eng.handle, kp, _ptr(offsets), nsets, bucket_size, leaf_size, flags, outs,
+                                   ctypes.byref(stats))
+    else:
+        raise ValueError(key_type)
+    _check(st, "build_batch")
+    funcs = [GPURecSplit(bucket_size=bucket_size, leaf_size=leaf_size, rotate=rotate, _handle=ctypes.c_void_p(outs[i]))
+             for i in range(nsets)]
+    return funcs, stats.as_dict()
 
 
 def hash_strings(keys, engine: Optional[Engine] = None) -> np.ndarray:

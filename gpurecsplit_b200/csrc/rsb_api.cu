@@ -87,6 +87,10 @@ struct rsb_engine {
     DBuf<uint8_t> nstage, bytes;
     DBuf<DevStatus> status;
     DBuf<EfParams> efp;
+    // batched construction
+    DBuf<uint64_t> set_key, set_bucket, set_bits, word_base, ef_base, out_block;
+    DBuf<uint32_t> set_nb, bucket_id, set_words, ef_words;
+    DBuf<EfParams> set_ef;
     cudaEvent_t ev[kNumEvents] = {};
 };
 
@@ -198,6 +202,42 @@ rsb_status copy_to_host(rsb_mphf *h, cudaStream_t st) {
     RSB_CK(cudaStreamSynchronize(st));
     h->host_valid = true;
     return RSB_OK;
+}
+
+// Every search stage in dependency order: fanout-2 depths, then each aggregation level
+// followed by its partition, then the leaves. Records the stage-boundary events.
+cudaError_t enqueue_searches(rsb_engine *e, const SearchCtx &sc, const LeafTables &lt, cudaStream_t st) {
+    cudaError_t err;
+    for (uint32_t d = 0; d < lt.max_higher_depth && d < (uint32_t)kMaxHigherDepth; ++d) {
+        search_higher(sc, (int)d, st);
+        if ((err = cudaEventRecord(e->ev[2 + d], st)) != cudaSuccess) return err;
+    }
+    for (int stage : {kStageUpper, kStageLower}) {
+        if ((err = cudaMemsetAsync(sc.slots, 0xFF, sc.nslots * sizeof(uint32_t), st)) != cudaSuccess) return err;
+        search_aggr(sc, stage, st);
+        partition_aggr(sc, stage, st);
+        if ((err = cudaEventRecord(e->ev[2 + stage], st)) != cudaSuccess) return err;
+    }
+    for (int stage : {kStageLeafRot, kStageLeafBF}) {
+        if ((err = cudaMemsetAsync(sc.slots, 0xFF, sc.nslots * sizeof(uint32_t), st)) != cudaSuccess) return err;
+        search_leaves(sc, stage, st);
+        if ((err = cudaEventRecord(e->ev[2 + stage], st)) != cudaSuccess) return err;
+    }
+    return cudaGetLastError();
+}
+
+// Per-stage device times of the last build from the engine's events.
+void fill_stage_times(rsb_engine *e, const LeafTables &lt, rsb_stats &S) {
+    S.ms_total = elapsed(e->ev[0], e->ev[kNumEvents - 1]);
+    S.ms_partition = elapsed(e->ev[0], e->ev[1]);
+    cudaEvent_t prev = e->ev[1];
+    for (int s = 0; s < kNumStages; ++s) {
+        const bool recorded = (s < (int)lt.max_higher_depth && s < kMaxHigherDepth) || s >= kStageUpper;
+        if (!recorded) continue;
+        S.ms_search[s] = elapsed(prev, e->ev[2 + s]);
+        prev = e->ev[2 + s];
+    }
+    S.ms_encode = elapsed(prev, e->ev[kNumEvents - 1]);
 }
 
 // The build proper. keys128 is device memory holding n (first, second) pairs.
@@ -322,22 +362,7 @@ rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint
     sc.budget_shift = e->budget_shift;
     sc.budget_min = e->budget_min;
     sc.num_sms = e->num_sms;
-    for (uint32_t d = 0; d < lt.max_higher_depth && d < (uint32_t)kMaxHigherDepth; ++d) {
-        search_higher(sc, (int)d, st);
-        RSB_CKH(cudaEventRecord(e->ev[2 + d], st));
-    }
-    for (int stage : {kStageUpper, kStageLower}) {
-        RSB_CKH(cudaMemsetAsync(e->slots.p, 0xFF, nslots * sizeof(uint32_t), st));
-        search_aggr(sc, stage, st);
-        partition_aggr(sc, stage, st);
-        RSB_CKH(cudaEventRecord(e->ev[2 + stage], st));
-    }
-    for (int stage : {kStageLeafRot, kStageLeafBF}) {
-        RSB_CKH(cudaMemsetAsync(e->slots.p, 0xFF, nslots * sizeof(uint32_t), st));
-        search_leaves(sc, stage, st);
-        RSB_CKH(cudaEventRecord(e->ev[2 + stage], st));
-    }
-    RSB_CKH(cudaGetLastError());
+    RSB_CKH(enqueue_searches(e, sc, lt, st));
 
     // ---- encoding ----
     launch_bucket_bits(e->node_base.p, nb, nodes, tab, e->bits.p, e->fixed_bits.p, e->status.p, st);
@@ -373,16 +398,7 @@ rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint
         tot += stage_counts[s];
     }
     S.nodes = tot;
-    S.ms_total = elapsed(e->ev[0], e->ev[kNumEvents - 1]);
-    S.ms_partition = elapsed(e->ev[0], e->ev[1]);
-    cudaEvent_t prev = e->ev[1];
-    for (int s = 0; s < kNumStages; ++s) {
-        const bool recorded = (s < (int)lt.max_higher_depth && s < kMaxHigherDepth) || s >= kStageUpper;
-        if (!recorded) continue;
-        S.ms_search[s] = elapsed(prev, e->ev[2 + s]);
-        prev = e->ev[2 + s];
-    }
-    S.ms_encode = elapsed(prev, e->ev[kNumEvents - 1]);
+    fill_stage_times(e, lt, S);
 
     if (keep_seeds) {
         h->seeds.resize(tot);
@@ -399,6 +415,205 @@ rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint
         if (s != RSB_OK) return fail(s);
     }
     *out = h;
+    return RSB_OK;
+}
+
+// Batched construction: nsets independent key sets (set s = keys [h_off[s], h_off[s+1]))
+// in one device pipeline. Sets share the global bucket space, so the tree, the stage lists
+// and every search kernel run once for all sets; bucket assignment and the encoders are
+// set-aware. outs[s] receives a host-side function identical to the plain build of set s.
+rsb_status build_batch_device(rsb_engine *e, const uint64_t *keys128, const uint64_t *h_off, uint32_t nsets,
+                              uint64_t bucket_size, uint32_t leaf, uint32_t flags, rsb_mphf **outs, rsb_stats *stats,
+                              const std::function<void()> &hash_keys) {
+    const bool rotate = (flags & RSB_ROTATE) != 0;
+    const LeafTables &lt = leaf_tables(leaf, rotate);
+    if (!shape_matches_kernels(lt.shape)) return RSB_ERR_INTERNAL;
+    DevTables tab;
+    rsb_status rs = get_device_tables(e, lt, leaf, rotate, tab);
+    if (rs != RSB_OK) return rs;
+    cudaStream_t st = e->stream;
+    const uint64_t n = h_off[nsets];
+    std::vector<uint64_t> set_nb(nsets);
+    uint64_t nb_total = 0, lower_cap = 0, cum_cap = 0, jump_cap = 0;
+    for (uint32_t s = 0; s < nsets; ++s) {
+        const uint64_t ns = h_off[s + 1] - h_off[s];
+        const uint64_t nb = std::max<uint64_t>(1, (ns + bucket_size - 1) / bucket_size);
+        set_nb[s] = nb;
+        nb_total += nb;
+        lower_cap += ((nb + 1) * 56 + 63) / 64 + 2;
+        cum_cap += (3 * (nb + 1) + 63) / 64 + 2;
+        jump_cap += jump_words_for(nb) + 2;
+    }
+    if (nb_total >= (1ull << 32) - 1) return RSB_ERR_BAD_ARG;
+    const uint64_t desc_cap = (8 * n) / 64 + 3 * (uint64_t)nsets + 16;
+    const uint64_t block_words = desc_cap + lower_cap + 2 * cum_cap + jump_cap;
+    const uint64_t max_nodes = n + 1;
+    const uint32_t nslots = search_slots_needed(e->num_sms);
+    RSB_ENSURE(e->sorted, n);
+    RSB_ENSURE(e->set_key, nsets + 1);
+    RSB_ENSURE(e->set_nb, nsets);
+    RSB_ENSURE(e->set_bucket, nsets + 1);
+    RSB_ENSURE(e->bucket_id, n);
+    RSB_ENSURE(e->counts, nb_total);
+    RSB_ENSURE(e->acc, nb_total + 1);
+    RSB_ENSURE(e->node_count, nb_total);
+    RSB_ENSURE(e->node_base, nb_total + 1);
+    RSB_ENSURE(e->scan_tmp, scan_blocks(std::max<uint64_t>(nb_total, nsets) + 1) + 8);
+    RSB_ENSURE(e->nstart, max_nodes);
+    RSB_ENSURE(e->nsize, max_nodes);
+    RSB_ENSURE(e->nstage, max_nodes);
+    RSB_ENSURE(e->seed, max_nodes);
+    RSB_ENSURE(e->nwin, max_nodes);
+    RSB_ENSURE(e->lists, max_nodes);
+    RSB_ENSURE(e->stage_info, 3 * kNumStages);
+    RSB_ENSURE(e->sched, kNumStages);
+    RSB_ENSURE(e->slots, nslots);
+    RSB_ENSURE(e->bits, nb_total);
+    RSB_ENSURE(e->fixed_bits, nb_total);
+    RSB_ENSURE(e->pos_acc, nb_total + 1);
+    RSB_ENSURE(e->status, 1);
+    RSB_ENSURE(e->efp, 1);
+    RSB_ENSURE(e->set_words, nsets);
+    RSB_ENSURE(e->set_bits, nsets);
+    RSB_ENSURE(e->word_base, nsets + 1);
+    RSB_ENSURE(e->ef_words, 4 * (uint64_t)nsets);
+    RSB_ENSURE(e->ef_base, 4 * ((uint64_t)nsets + 1));
+    RSB_ENSURE(e->set_ef, nsets);
+    RSB_ENSURE(e->out_block, block_words);
+
+    NodeArrays nodes{e->nstart.p, e->nsize.p, e->nstage.p, e->seed.p, e->nwin.p};
+    ScanTmp stmp{e->scan_tmp.p, e->scan_tmp.cap};
+    const uint64_t *node_total = e->node_base.p + nb_total;
+    const uint64_t launches0 = launches_so_far();
+    uint64_t *desc = e->out_block.p, *lower = desc + desc_cap, *ucum = lower + lower_cap, *upos = ucum + cum_cap,
+             *jump = upos + cum_cap;
+    uint32_t *lw = e->ef_words.p, *cw = lw + nsets, *pw = cw + nsets, *jw = pw + nsets;
+    uint64_t *lb = e->ef_base.p, *cb = lb + nsets + 1, *pb = cb + nsets + 1, *jb = pb + nsets + 1;
+
+    RSB_CK(cudaEventRecord(e->ev[0], st));
+    if (hash_keys) hash_keys();
+    RSB_CK(cudaMemsetAsync(e->status.p, 0, sizeof(DevStatus), st));
+    RSB_CK(cudaMemsetAsync(e->efp.p, 0, sizeof(EfParams), st));
+    RSB_CK(cudaMemsetAsync(e->sched.p, 0, kNumStages * sizeof(uint32_t), st));
+    RSB_CK(cudaMemcpyAsync(e->set_key.p, h_off, (nsets + 1) * 8, cudaMemcpyHostToDevice, st));
+    // ---- buckets of all sets ----
+    launch_set_nbuckets(e->set_key.p, nsets, bucket_size, e->set_nb.p, st);
+    exclusive_scan_u32(e->set_nb.p, e->set_bucket.p, nsets, stmp, st);
+    launch_set_bucket_ids(keys128, n, e->set_key.p, e->set_bucket.p, nsets, nb_total, e->bucket_id.p, e->counts.p, st);
+    launch_bucket_check(e->counts.p, nb_total, e->status.p, st);
+    exclusive_scan_u32(e->counts.p, e->acc.p, nb_total, stmp, st);
+    launch_set_scatter(keys128, n, e->bucket_id.p, e->acc.p, e->counts.p, nb_total, e->sorted.p, st);
+    launch_bucket_sort(e->sorted.p, e->acc.p, nb_total, e->status.p, st);
+    // ---- tree ----
+    launch_bucket_nodes(e->acc.p, nb_total, tab, e->node_count.p, st);
+    exclusive_scan_u32(e->node_count.p, e->node_base.p, nb_total, stmp, st);
+    RSB_CK(cudaMemsetAsync(e->seed.p, 0xFF, max_nodes * sizeof(uint64_t), st));
+    RSB_CK(cudaMemsetAsync(e->nwin.p, 0, max_nodes * sizeof(uint32_t), st));
+    launch_tree_emit(e->acc.p, nb_total, e->node_base.p, lt.shape, nodes, st);
+    launch_stage_lists(e->nstage.p, node_total, (uint32_t)max_nodes, e->stage_info.p, e->lists.p, st);
+    RSB_CK(cudaGetLastError());
+    RSB_CK(cudaEventRecord(e->ev[1], st));
+    // ---- searches (all sets at once) ----
+    SearchCtx sc{};
+    sc.sh = lt.shape;
+    sc.node_total = node_total;
+    sc.stage_info = e->stage_info.p;
+    sc.lists = e->lists.p;
+    sc.nodes = nodes;
+    sc.keys = e->sorted.p;
+    sc.tab = tab;
+    sc.status = e->status.p;
+    sc.sched = e->sched.p;
+    sc.slots = e->slots.p;
+    sc.nslots = nslots;
+    sc.budget_shift = e->budget_shift;
+    sc.budget_min = e->budget_min;
+    sc.num_sms = e->num_sms;
+    RSB_CK(enqueue_searches(e, sc, lt, st));
+    // ---- per-set encoding ----
+    launch_bucket_bits(e->node_base.p, nb_total, nodes, tab, e->bits.p, e->fixed_bits.p, e->status.p, st);
+    exclusive_scan_u32(e->bits.p, e->pos_acc.p, nb_total, stmp, st);
+    launch_set_desc_words(e->pos_acc.p, e->set_bucket.p, nsets, e->set_words.p, e->set_bits.p, st);
+    exclusive_scan_u32(e->set_words.p, e->word_base.p, nsets, stmp, st);
+    RSB_CK(cudaMemsetAsync(e->out_block.p, 0, block_words * 8, st));
+    launch_set_write_rice(e->node_base.p, nb_total, nodes, tab, e->pos_acc.p, e->fixed_bits.p, e->set_bucket.p, nsets,
+                          e->word_base.p, e->set_bits.p, desc, desc_cap, e->status.p, st);
+    launch_set_ef_params(e->acc.p, e->pos_acc.p, e->set_bucket.p, nsets, e->set_ef.p, lw, cw, pw, jw, st);
+    exclusive_scan_u32(lw, lb, nsets, stmp, st);
+    exclusive_scan_u32(cw, cb, nsets, stmp, st);
+    exclusive_scan_u32(pw, pb, nsets, stmp, st);
+    exclusive_scan_u32(jw, jb, nsets, stmp, st);
+    launch_set_ef_fill(e->acc.p, e->pos_acc.p, e->set_bucket.p, nsets, e->set_ef.p, lb, cb, pb, jb, lower, ucum, upos,
+                       jump, st);
+    launch_evals(node_total, nodes, leaf, rotate ? 1 : 0, e->efp.p, st);
+    RSB_CK(cudaGetLastError());
+    RSB_CK(cudaEventRecord(e->ev[kNumEvents - 1], st));
+
+    DevStatus dst{};
+    EfParams totals{};
+    uint32_t stage_counts[kNumStages];
+    std::vector<EfParams> sef(nsets);
+    std::vector<uint64_t> bases(4 * ((uint64_t)nsets + 1)), wbase(nsets + 1);
+    RSB_CK(cudaMemcpyAsync(&dst, e->status.p, sizeof(dst), cudaMemcpyDeviceToHost, st));
+    RSB_CK(cudaMemcpyAsync(&totals, e->efp.p, sizeof(totals), cudaMemcpyDeviceToHost, st));
+    RSB_CK(cudaMemcpyAsync(stage_counts, e->stage_info.p, sizeof(stage_counts), cudaMemcpyDeviceToHost, st));
+    if (nsets) {
+        RSB_CK(cudaMemcpyAsync(sef.data(), e->set_ef.p, nsets * sizeof(EfParams), cudaMemcpyDeviceToHost, st));
+        RSB_CK(cudaMemcpyAsync(bases.data(), e->ef_base.p, bases.size() * 8, cudaMemcpyDeviceToHost, st));
+        RSB_CK(cudaMemcpyAsync(wbase.data(), e->word_base.p, wbase.size() * 8, cudaMemcpyDeviceToHost, st));
+    }
+    RSB_CK(cudaStreamSynchronize(st));
+    if (dst.code != 0) return (rsb_status)dst.code;
+    // the used part of each output array, then one function per set
+    std::vector<uint64_t> hdesc(nsets ? wbase[nsets] : 0), hlower(nsets ? bases[nsets] : 0),
+        hcum(nsets ? bases[2 * (nsets + 1) - 1] : 0), hpos(nsets ? bases[3 * (nsets + 1) - 1] : 0),
+        hjump(nsets ? bases[4 * (nsets + 1) - 1] : 0);
+    if (!hdesc.empty()) RSB_CK(cudaMemcpyAsync(hdesc.data(), desc, hdesc.size() * 8, cudaMemcpyDeviceToHost, st));
+    if (!hlower.empty()) RSB_CK(cudaMemcpyAsync(hlower.data(), lower, hlower.size() * 8, cudaMemcpyDeviceToHost, st));
+    if (!hcum.empty()) RSB_CK(cudaMemcpyAsync(hcum.data(), ucum, hcum.size() * 8, cudaMemcpyDeviceToHost, st));
+    if (!hpos.empty()) RSB_CK(cudaMemcpyAsync(hpos.data(), upos, hpos.size() * 8, cudaMemcpyDeviceToHost, st));
+    if (!hjump.empty()) RSB_CK(cudaMemcpyAsync(hjump.data(), jump, hjump.size() * 8, cudaMemcpyDeviceToHost, st));
+    RSB_CK(cudaStreamSynchronize(st));
+    const uint64_t *hlb = bases.data(), *hcb = hlb + nsets + 1, *hpb = hcb + nsets + 1, *hjb = hpb + nsets + 1;
+    for (uint32_t s = 0; s < nsets; ++s) {
+        auto *h = new (std::nothrow) rsb_mphf;
+        if (!h) {
+            for (uint32_t t = 0; t < s; ++t) rsb_free(outs[t]);
+            return RSB_ERR_OOM;
+        }
+        h->leaf = leaf;
+        h->rotate = rotate;
+        h->bucket_size = bucket_size;
+        h->keys_count = h_off[s + 1] - h_off[s];
+        h->nbuckets = set_nb[s];
+        h->tab = &lt;
+        h->ef = sef[s];
+        h->desc.assign(hdesc.begin() + wbase[s], hdesc.begin() + wbase[s + 1]);
+        h->lower.assign(hlower.begin() + hlb[s], hlower.begin() + hlb[s + 1]);
+        h->upper_cum.assign(hcum.begin() + hcb[s], hcum.begin() + hcb[s + 1]);
+        h->upper_pos.assign(hpos.begin() + hpb[s], hpos.begin() + hpb[s + 1]);
+        h->jump.assign(hjump.begin() + hjb[s], hjump.begin() + hjb[s + 1]);
+        h->host_valid = true;
+        h->stats.keys = h->keys_count;
+        h->stats.buckets = set_nb[s];
+        h->stats.descriptor_bits = sef[s].total_bits;
+        outs[s] = h;
+    }
+    if (stats) {
+        rsb_stats &S = *stats;
+        S = rsb_stats{};
+        S.keys = n;
+        S.buckets = nb_total;
+        S.evals_alg = totals.evals_alg;
+        for (int s = 0; s < kNumStages; ++s) {
+            S.evals_stage[s] = totals.evals_stage[s];
+            S.nodes_per_stage[s] = stage_counts[s];
+            S.nodes += stage_counts[s];
+        }
+        S.kernel_launches = launches_so_far() - launches0;
+        for (uint32_t s = 0; s < nsets; ++s) S.descriptor_bits += sef[s].total_bits;
+        fill_stage_times(e, lt, S);
+    }
     return RSB_OK;
 }
 
@@ -506,6 +721,9 @@ rsb_status rsb_engine_destroy(rsb_engine *e) {
     release(e->node_count); release(e->lists); release(e->stage_info); release(e->sched); release(e->slots);
     release(e->bits); release(e->fixed_bits); release(e->nstart); release(e->nwin); release(e->nsize);
     release(e->nstage); release(e->bytes); release(e->status); release(e->efp);
+    release(e->set_key); release(e->set_bucket); release(e->set_bits); release(e->word_base); release(e->ef_base);
+    release(e->out_block); release(e->set_nb); release(e->bucket_id); release(e->set_words); release(e->ef_words);
+    release(e->set_ef);
     for (auto &kv : e->tables) cudaFree(kv.second.first);
     for (auto &ev : e->ev) cudaEventDestroy(ev);
     if (e->own_stream) cudaStreamDestroy(e->stream);
@@ -597,6 +815,55 @@ rsb_status rsb_build_strings(rsb_engine *e, const uint8_t *bytes, const uint64_t
     cudaStream_t st = e->stream;
     return build_device(e, k128, n, bucket_size, leaf, flags, out, (flags & kKeepSeeds) != 0,
                         [=] { launch_hash_strings(db, doff, n, k128, st); });
+}
+
+static rsb_status check_batch(rsb_engine *e, const uint64_t *set_offsets, uint32_t nsets, uint64_t bucket_size,
+                              uint32_t leaf, rsb_mphf **outs) {
+    if (!e || !set_offsets || (nsets && !outs)) return RSB_ERR_BAD_ARG;
+    if (leaf < 2 || leaf > (uint32_t)kMaxLeafSize || bucket_size == 0) return RSB_ERR_BAD_ARG;
+    if (set_offsets[0] != 0) return RSB_ERR_BAD_ARG;
+    for (uint32_t s = 0; s < nsets; ++s)
+        if (set_offsets[s + 1] < set_offsets[s]) return RSB_ERR_BAD_ARG;
+    if (set_offsets[nsets] >= (1ull << 32) - 1) return RSB_ERR_BAD_ARG;
+    if (cudaSetDevice(e->device) != cudaSuccess) {
+        cudaGetLastError();
+        return RSB_ERR_CUDA;
+    }
+    return RSB_OK;
+}
+
+rsb_status rsb_build_batch_hash128(rsb_engine *e, const rsb_hash128 *keys, const uint64_t *set_offsets, uint32_t nsets,
+                                   uint64_t bucket_size, uint32_t leaf, uint32_t flags, rsb_mphf **outs,
+                                   rsb_stats *stats) {
+    rsb_status s = check_batch(e, set_offsets, nsets, bucket_size, leaf, outs);
+    if (s != RSB_OK) return s;
+    const uint64_t n = set_offsets[nsets];
+    if (n && !keys) return RSB_ERR_BAD_ARG;
+    const uint64_t *dk = nullptr;
+    s = stage_keys128(e, keys, n, flags, &dk);
+    if (s != RSB_OK) return s;
+    return build_batch_device(e, dk, set_offsets, nsets, bucket_size, leaf, flags, outs, stats, std::function<void()>());
+}
+
+rsb_status rsb_build_batch_u64(rsb_engine *e, const uint64_t *keys, const uint64_t *set_offsets, uint32_t nsets,
+                               uint64_t bucket_size, uint32_t leaf, uint32_t flags, rsb_mphf **outs, rsb_stats *stats) {
+    rsb_status s = check_batch(e, set_offsets, nsets, bucket_size, leaf, outs);
+    if (s != RSB_OK) return s;
+    const uint64_t n = set_offsets[nsets];
+    if (n && !keys) return RSB_ERR_BAD_ARG;
+    const uint64_t *dk = keys;
+    if (!(flags & RSB_KEYS_ON_DEVICE)) {
+        s = ensure(e->raw_u64, n);
+        if (s != RSB_OK) return s;
+        if (n) RSB_CK(cudaMemcpyAsync(e->raw_u64.p, keys, n * 8, cudaMemcpyHostToDevice, e->stream));
+        dk = e->raw_u64.p;
+    }
+    s = ensure(e->keys128, 2 * n);
+    if (s != RSB_OK) return s;
+    uint64_t *k128 = e->keys128.p;
+    cudaStream_t st = e->stream;
+    return build_batch_device(e, k128, set_offsets, nsets, bucket_size, leaf, flags, outs, stats,
+                              [=] { launch_hash_u64(dk, n, k128, st); });
 }
 
 rsb_status rsb_hash_strings(rsb_engine *e, const uint8_t *bytes, const uint64_t *offsets, uint64_t n, uint32_t flags,

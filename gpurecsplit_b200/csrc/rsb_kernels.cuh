@@ -90,6 +90,26 @@ void launch_ef_build(const uint64_t *cum, const uint64_t *pos, uint64_t nbuckets
 void launch_evals(const uint64_t *node_total, NodeArrays nodes, uint32_t leaf, uint32_t rotate, EfParams *ef,
                   cudaStream_t st);
 
+// ---- batched construction (rsb_batch.cu) ----
+void launch_set_nbuckets(const uint64_t *set_key, uint32_t nsets, uint64_t bucket_size, uint32_t *nb, cudaStream_t st);
+void launch_set_bucket_ids(const uint64_t *keys128, uint64_t n, const uint64_t *set_key, const uint64_t *set_bucket,
+                           uint32_t nsets, uint64_t nb_total, uint32_t *bucket_id, uint32_t *counts, cudaStream_t st);
+void launch_set_scatter(const uint64_t *keys128, uint64_t n, const uint32_t *bucket_id, const uint64_t *acc,
+                        uint32_t *cursor, uint64_t nb_total, uint64_t *sorted, cudaStream_t st);
+void launch_set_desc_words(const uint64_t *pos_acc, const uint64_t *set_bucket, uint32_t nsets, uint32_t *words,
+                           uint64_t *set_bits, cudaStream_t st);
+void launch_set_write_rice(const uint64_t *node_base, uint64_t nb_total, NodeArrays nodes, DevTables tab,
+                           const uint64_t *pos_acc, const uint32_t *fixed_bits, const uint64_t *set_bucket,
+                           uint32_t nsets, const uint64_t *word_base, const uint64_t *set_bits, uint64_t *desc,
+                           uint64_t cap_words, DevStatus *status, cudaStream_t st);
+void launch_set_ef_params(const uint64_t *acc, const uint64_t *pos, const uint64_t *set_bucket, uint32_t nsets,
+                          EfParams *ef, uint32_t *lower_w, uint32_t *cum_w, uint32_t *pos_w, uint32_t *jump_w,
+                          cudaStream_t st);
+void launch_set_ef_fill(const uint64_t *acc, const uint64_t *pos, const uint64_t *set_bucket, uint32_t nsets,
+                        const EfParams *ef, const uint64_t *lower_base, const uint64_t *cum_base, const uint64_t *pos_base,
+                        const uint64_t *jump_base, uint64_t *lower, uint64_t *upper_cum, uint64_t *upper_pos,
+                        uint64_t *jump, cudaStream_t st);
+
 // ---- queries (rsb_query.cu) ----
 struct MphfView;
 void launch_query_view(const MphfView &f, const uint64_t *keys128, uint64_t n, uint64_t *out, cudaStream_t st);

@@ -113,12 +113,16 @@ __device__ uint32_t find_help(const SearchCtx &c, uint32_t start) {
 // Fanout-2 nodes: one CTA per node, search and stable 2-way partition.
 // remap(k + x, m) < split  <=>  hash16(k + x) < ceil(split * 2^16 / m).
 // ---------------------------------------------------------------------------------------
-constexpr int kHigherSeedsPerThread = 2;
+// A node needs about sqrt(2*pi*m*p*(1-p)) (tens of) seeds, so small CTAs keep the
+// last window's overshoot small: 64 threads, one seed each per window.
+constexpr int kHigherThreads = 64;
+constexpr int kHigherWarps = kHigherThreads / 32;
+constexpr int kHigherSeedsPerThread = 1;
 
-__global__ void __launch_bounds__(kThreads) k_search_higher(SearchCtx c, int depth) {
+__global__ void __launch_bounds__(kHigherThreads) k_search_higher(SearchCtx c, int depth) {
     extern __shared__ uint64_t sk[];
     __shared__ unsigned long long s_best;
-    __shared__ uint32_t s_warp[kWarpsPerCta];
+    __shared__ uint32_t s_warp[kHigherWarps];
     __shared__ int s_stop;
     const uint32_t count = c.stage_info[depth];
     const uint32_t base = c.stage_info[kNumStages + depth];
@@ -134,16 +138,16 @@ __global__ void __launch_bounds__(kThreads) k_search_higher(SearchCtx c, int dep
         const uint32_t m = c.nodes.size[id];
         const uint32_t split = upper * (uint16_t(m / 2 + upper - 1) / upper);
         const uint32_t thr = (uint32_t)((((uint64_t)split << 16) + m - 1) / m);
-        for (uint32_t i = threadIdx.x; i < m; i += kThreads) sk[i] = c.keys[start + i];
+        for (uint32_t i = threadIdx.x; i < m; i += kHigherThreads) sk[i] = c.keys[start + i];
         if (threadIdx.x == 0) s_best = kSeedNotFound;
         __syncthreads();
         const uint64_t budget = budget_for(c, m);
-        constexpr uint32_t W = kThreads * kHigherSeedsPerThread;
+        constexpr uint32_t W = kHigherThreads * kHigherSeedsPerThread;
         bool failed = false;
         for (uint64_t x0 = 0;; x0 += W) {
 #pragma unroll
             for (int s = 0; s < kHigherSeedsPerThread; ++s) {
-                const uint64_t x = x0 + threadIdx.x + (uint64_t)s * kThreads;
+                const uint64_t x = x0 + threadIdx.x + (uint64_t)s * kHigherThreads;
                 const uint64_t sx = seed + x;
                 uint32_t cnt = 0;
                 for (uint32_t i = 0; i < m; ++i) cnt += hash16(sk[i] + sx) < thr;
@@ -165,7 +169,7 @@ __global__ void __launch_bounds__(kThreads) k_search_higher(SearchCtx c, int dep
             return;
         }
         // Stable partition: keys remapping below `split` first (SIMDRecSplit.hpp:288-306).
-        const uint32_t per = (m + kThreads - 1) / kThreads;
+        const uint32_t per = (m + kHigherThreads - 1) / kHigherThreads;
         const uint32_t b0 = min(m, threadIdx.x * per), b1 = min(m, b0 + per);
         const uint64_t sx = seed + x;
         uint32_t left = 0;
@@ -611,9 +615,9 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
 // ---- host-side dispatch -------------------------------------------------------------
 
 template <typename K>
-int persistent_grid(K kernel, size_t smem, int num_sms) {
+int persistent_grid(K kernel, size_t smem, int num_sms, int threads = kThreads) {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
     if (per_sm < 1) per_sm = 1;
     return per_sm * num_sms;
 }
@@ -713,7 +717,8 @@ bool shape_matches_kernels(const Shape &s) { return s.lower == lower_of((int)s.l
 void search_higher(const SearchCtx &c, int depth, cudaStream_t st) {
     const size_t smem = kMaxBucketSize * sizeof(uint64_t);
     cudaFuncSetAttribute(k_search_higher, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_search_higher<<<persistent_grid(k_search_higher, smem, c.num_sms), kThreads, smem, st>>>(c, depth);
+    k_search_higher<<<persistent_grid(k_search_higher, smem, c.num_sms, kHigherThreads), kHigherThreads, smem, st>>>(c,
+                                                                                                           depth);
     count_launches(1);
 }
 
@@ -731,28 +736,30 @@ void search_leaves(const SearchCtx &c, int stage, cudaStream_t st) {
 }
 
 // ---- eval-rate probe ------------------------------------------------------------------
-// The cheapest complete candidate evaluation of any search (64-bit add, remix32, 16-bit
-// threshold compare, count), laid out like the search kernels (keys broadcast from shared
-// memory, four independent candidates per lane) with no scheduling, no reductions and no
-// early exit: the integer ceiling for remixAndRemap32 evaluations on this device.
+// The cheapest complete candidate evaluation of any search (key + seed, remix32, 16-bit
+// threshold compare, count) in the exact form of the aggregation filter (threshold_counts:
+// keys broadcast from shared memory, 8 candidates per lane, unrolled key loop), run at full
+// occupancy with no scheduling, no queues and no reductions: the integer ceiling for
+// remixAndRemap32 evaluations on this device.
 namespace {
 constexpr int kProbeKeys = 128;
-constexpr int kProbeIters = 64;
+constexpr int kProbeIters = 32;
+constexpr int kProbeSeeds = 8;
 __global__ void __launch_bounds__(kThreads) k_probe(unsigned long long *sink) {
     __shared__ uint64_t sk[kProbeKeys];
     for (int i = threadIdx.x; i < kProbeKeys; i += kThreads) sk[i] = start_seed(i % 20) * (2 * i + 1);
     __syncthreads();
-    uint32_t cnt[4] = {0, 0, 0, 0};
-    uint64_t bx = start_seed(17) + blockIdx.x * (uint64_t)kThreads + threadIdx.x;
-    for (int it = 0; it < kProbeIters; ++it) {
-        for (int i = 0; i < kProbeKeys; ++i) {
-            const uint64_t t = sk[i] + bx;
+    uint32_t cnt[kProbeSeeds];
 #pragma unroll
-            for (int s = 0; s < 4; ++s) cnt[s] += hash16(t + 32u * s) < 30001u;
-        }
-        bx += 1ull << 32;
+    for (int s = 0; s < kProbeSeeds; ++s) cnt[s] = 0;
+    uint64_t bu = start_seed(17) + (blockIdx.x * (uint64_t)kWarpsPerCta + (threadIdx.x >> 5)) * 32 * kProbeSeeds;
+    for (int it = 0; it < kProbeIters; ++it) {
+        threshold_counts<kProbeSeeds>(sk, kProbeKeys, bu, 30001u, cnt);
+        bu += 1ull << 32;
     }
-    const uint32_t tot = cnt[0] + cnt[1] + cnt[2] + cnt[3];
+    uint32_t tot = 0;
+#pragma unroll
+    for (int s = 0; s < kProbeSeeds; ++s) tot += cnt[s];
     if (tot == 0xFFFFFFFFu) atomicAdd(sink, 1ull);  // keeps the loop alive
 }
 }  // namespace
@@ -764,7 +771,7 @@ void probe_eval_rate(int num_sms, uint64_t *out_evals, cudaStream_t st) {
     k_probe<<<g, kThreads, 0, st>>>(sink);
     cudaFreeAsync(sink, st);
     count_launches(1);
-    *out_evals = (uint64_t)g * kThreads * kProbeIters * kProbeKeys * 4;
+    *out_evals = (uint64_t)g * kThreads * kProbeIters * kProbeKeys * kProbeSeeds;
 }
 
 }  // namespace rsb

@@ -101,6 +101,19 @@ rsb_status rsb_build_strings(rsb_engine *engine, const uint8_t *bytes, const uin
 rsb_status rsb_build_u64(rsb_engine *engine, const uint64_t *keys, uint64_t n, uint64_t bucket_size,
                          uint32_t leaf_size, uint32_t flags, rsb_mphf **out);
 
+/* Batched construction (no reference counterpart: the reference builds one set per
+ * constructor call). Builds nsets independent functions in one device pipeline; set s is
+ * keys[set_offsets[s] .. set_offsets[s+1]) (set_offsets: host memory, nsets + 1 entries,
+ * starting at 0, non-decreasing). outs[s] is identical to the plain build of set s with the
+ * same bucket size, leaf size and flags; it lives on the host. `stats` (may be NULL)
+ * receives the whole batch's measurements. */
+rsb_status rsb_build_batch_hash128(rsb_engine *engine, const rsb_hash128 *keys, const uint64_t *set_offsets,
+                                   uint32_t nsets, uint64_t bucket_size, uint32_t leaf_size, uint32_t flags,
+                                   rsb_mphf **outs, rsb_stats *stats);
+rsb_status rsb_build_batch_u64(rsb_engine *engine, const uint64_t *keys, const uint64_t *set_offsets, uint32_t nsets,
+                               uint64_t bucket_size, uint32_t leaf_size, uint32_t flags, rsb_mphf **outs,
+                               rsb_stats *stats);
+
 /* ---- queries and accessors --------------------------------------------------------- */
 
 /* Replaces size_t operator()(const hash128_t&), AbstractParallelRecSplit.hpp:409-466
