@@ -390,6 +390,137 @@ def run_batch(args) -> None:
     engine.close()
 
 
+# ---------------------------------------------------------------------------------------
+# Serving form: continuous batching of string-key build requests under an HBM budget
+# ---------------------------------------------------------------------------------------
+SERVE_CLASSES = [(8, 100), (12, 1000), (16, 2000)]
+
+
+def string_pool(n: int, seed: int = 2024):
+    """n random byte strings of 10..50 bytes (numpy default_rng(seed)), concatenated."""
+    rng = np.random.default_rng(seed)
+    lens = rng.integers(10, 51, n)
+    offsets = np.zeros(n + 1, dtype=np.uint64)
+    offsets[1:] = np.cumsum(lens)
+    data = rng.integers(0, 256, int(offsets[-1]), dtype=np.uint8)
+    return data, offsets
+
+
+def serve_requests(nreq: int, pool_n: int, max_keys: int, seed: int = 11):
+    """Request i: size round(exp(U[ln 100, ln max_keys])), class uniform over (l, b), a
+    contiguous slice of the string pool at a uniform offset."""
+    rng = np.random.default_rng(seed)
+    sizes = np.rint(np.exp(rng.uniform(np.log(100), np.log(max_keys), nreq))).astype(np.int64)
+    cls = rng.integers(0, len(SERVE_CLASSES), nreq)
+    starts = [int(rng.integers(0, pool_n - s + 1)) for s in sizes]
+    return [(int(st), int(sz), SERVE_CLASSES[c]) for st, sz, c in zip(starts, sizes, cls)]
+
+
+def run_serve(args) -> None:
+    import threading
+
+    import torch
+    import gpurecsplit_b200 as rsb
+
+    torch.cuda.set_device(0)
+    data, offsets = string_pool(args.max_keys)
+    reqs = serve_requests(args.requests, args.max_keys, args.max_keys)
+    total_keys = sum(r[1] for r in reqs)
+
+    def keys_of(r):
+        st, n, _ = r
+        return data, offsets[st:st + n + 1]
+
+    def submit(srv, r):
+        _, _, (leaf, b) = r
+        return srv.submit_strings(keys_of(r), b, leaf)
+
+    srv = rsb.Server(hbm_budget=args.hbm_budget, inflight=args.inflight)
+    # Warm-up: 1M-key requests of every class on every worker size the engines' scratch.
+    wn = min(1_000_000, args.max_keys)
+    warm = [srv.submit_strings((data, offsets[:wn + 1]), b, leaf)
+            for _ in range(args.inflight) for leaf, b in SERVE_CLASSES]
+    for w in warm:
+        srv.wait(w)
+
+    with ClockSampler(0) as clocks:
+        # Saturated leg: every request queued at once -> capacity.
+        t0 = time.perf_counter()
+        ids = [submit(srv, r) for r in reqs]
+        sat = [srv.wait(i) for i in ids]
+        t_sat = time.perf_counter() - t0
+        capacity = total_keys / t_sat
+
+        # Poisson leg at `load` x capacity (arrival rate in requests/s).
+        rate = args.load * capacity / (total_keys / len(reqs))
+        gaps = np.random.default_rng(5).exponential(1.0 / rate, len(reqs))
+        ids = [None] * len(reqs)
+        lag = []
+
+        def submitter():
+            start = time.perf_counter()
+            t_next = 0.0
+            for i, r in enumerate(reqs):
+                t_next += gaps[i]
+                d = t_next - (time.perf_counter() - start)
+                if d > 0:
+                    time.sleep(d)
+                lag.append(max(0.0, -d))
+                ids[i] = submit(srv, r)
+
+        th = threading.Thread(target=submitter)
+        t1 = time.perf_counter()
+        th.start()
+        th.join()
+        poi = [srv.wait(i) for i in ids]
+        t_poi = time.perf_counter() - t1
+    srv.close()
+
+    lat = np.array([(info["done_s"] - info["submit_s"]) * 1e3 for _, info in poi])
+    qwait = np.array([(info["admit_s"] - info["submit_s"]) * 1e3 for _, info in poi])
+    batch_req = np.array([info["batch_requests"] for _, info in poi])
+
+    # Each request alone (plain build, one engine, back to back): identity + sequential rate.
+    engine = rsb.Engine(0)
+    same = True
+    t2 = time.perf_counter()
+    for r, (fs, _), (fp, _) in zip(reqs, sat, poi):
+        _, _, (leaf, b) = r
+        alone = rsb.GPURecSplit(keys_of(r), bucket_size=b, leaf_size=leaf, key_type="strings", engine=engine)
+        blob = alone.serialize()
+        same &= blob == fs.serialize() and blob == fp.serialize()
+        alone.close()
+    t_alone = time.perf_counter() - t2
+    engine.close()
+
+    per_class = {}
+    for (st, n, (leaf, b)), l_ms in zip(reqs, lat):
+        per_class.setdefault(f"l={leaf},b={b}", []).append(l_ms)
+    line = {
+        "metric": "serve keys/s (string requests, log-uniform [100,1e7] keys, mixed (l,b))",
+        "value": capacity, "unit": "keys/s", "higher_is_better": True, "n_gpus": 1, "steps": 1, "warmup": 1,
+        "ms_per_step": t_sat * 1e3, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": f"{len(reqs)} requests; size round(exp(U[ln 100, ln {args.max_keys:.0e}])), "
+                               f"(l,b) uniform over {SERVE_CLASSES}, keys = slices of a pool of {args.max_keys} "
+                               "random 10-50 byte strings (numpy seed 2024), rotation",
+                   "requests": len(reqs), "keys": total_keys, "hbm_budget": args.hbm_budget,
+                   "inflight": args.inflight, "timing": "host wall clock (server steady clock for latency)"},
+        "saturated": {"keys_per_s": capacity, "s": t_sat,
+                      "mean_batch_requests": float(np.mean([i["batch_requests"] for _, i in sat]))},
+        "poisson": {"load": args.load, "rate_req_per_s": rate, "keys_per_s": total_keys / t_poi, "s": t_poi,
+                    "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                    "queue_p50_ms": float(np.percentile(qwait, 50)), "queue_p99_ms": float(np.percentile(qwait, 99)),
+                    "mean_batch_requests": float(batch_req.mean()), "max_submit_lag_ms": 1e3 * max(lag),
+                    "p50_ms_by_class": {k: float(np.percentile(v, 50)) for k, v in per_class.items()},
+                    "p99_ms_by_class": {k: float(np.percentile(v, 99)) for k, v in per_class.items()}},
+        "alone_back_to_back": {"keys_per_s": total_keys / t_alone, "s": t_alone},
+        "speedup_vs_alone": t_alone / t_sat,
+        "identical_to_alone": bool(same),
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -400,11 +531,19 @@ def main() -> None:
     ap.add_argument("--cpu-buckets", type=int, default=48)
     ap.add_argument("--ref-buckets", type=int, default=24)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="plain", choices=["plain", "batch"])
+    ap.add_argument("--mode", default="plain", choices=["plain", "batch", "serve"])
     ap.add_argument("--sets", type=int, default=1000)
+    ap.add_argument("--requests", type=int, default=100)
+    ap.add_argument("--max-keys", type=int, default=10_000_000)
+    ap.add_argument("--hbm-budget", type=int, default=32 << 30)
+    ap.add_argument("--inflight", type=int, default=2)
+    ap.add_argument("--load", type=float, default=0.75)
     args = ap.parse_args()
     if args.mode == "batch":
         run_batch(args)
+        return
+    if args.mode == "serve":
+        run_serve(args)
         return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

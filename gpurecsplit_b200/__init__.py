@@ -63,6 +63,11 @@ class Stats(ctypes.Structure):
         }
 
 
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("submit_s", ctypes.c_double), ("admit_s", ctypes.c_double), ("done_s", ctypes.c_double),
+                ("batch_requests", ctypes.c_uint32), ("batch_keys", ctypes.c_uint64)]
+
+
 def build_library() -> str:
     from . import build as _build
     return _build.build()
@@ -102,6 +107,12 @@ def lib():
             "rsb_hash_strings_static": ([vp, vp, u64, vp, vp], i32),
             "rsb_build_batch_hash128": ([vp, vp, vp, u32, u64, u32, u32, vp, ctypes.POINTER(Stats)], i32),
             "rsb_build_batch_u64": ([vp, vp, vp, u32, u64, u32, u32, vp, ctypes.POINTER(Stats)], i32),
+            "rsb_build_batch_strings": ([vp, vp, vp, vp, u32, u64, u32, u32, vp, ctypes.POINTER(Stats)], i32),
+            "rsb_server_create": ([i32, u64, u32, u64, pp], i32),
+            "rsb_server_submit_strings": ([vp, vp, vp, u64, u64, u32, u32, ctypes.POINTER(u64)], i32),
+            "rsb_server_submit_hash128": ([vp, vp, u64, u64, u32, u32, ctypes.POINTER(u64)], i32),
+            "rsb_server_wait": ([vp, u64, ctypes.c_double, pp, ctypes.POINTER(RequestInfo)], i32),
+            "rsb_server_destroy": ([vp], i32),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -327,9 +338,11 @@ def build_batch(keys: np.ndarray, set_offsets, bucket_size: int, leaf_size: int,
                 n_keys: Optional[int] = None):
     """Builds one function per key set in a single device pipeline (rsb_build_batch_*).
 
-    Set s is keys[set_offsets[s]:set_offsets[s+1]]. ``keys`` is a (n, 2) uint64 hash128 array
-    or (``key_type="u64"``) a uint64 array, or with ``keys_on_device`` a device pointer (int).
-    Returns (list of GPURecSplit, stats dict); each function equals the plain build of its set.
+    Set s is keys[set_offsets[s]:set_offsets[s+1]]. ``keys`` is a (n, 2) uint64 hash128 array,
+    (``key_type="u64"``) a uint64 array, (``key_type="strings"``) a (bytes, offsets) pair of
+    uint8/uint64 arrays or a sequence of str/bytes, or with ``keys_on_device`` a device
+    pointer (int). Returns (list of GPURecSplit, stats dict); each function equals the plain
+    build of its set.
     """
     eng = engine or default_engine()
     offsets = np.ascontiguousarray(set_offsets, dtype=np.uint64)
@@ -338,6 +351,19 @@ def build_batch(keys: np.ndarray, set_offsets, bucket_size: int, leaf_size: int,
     stats = Stats()
     flags = (RSB_ROTATE if rotate else 0) | (RSB_KEYS_ON_DEVICE if keys_on_device else 0)
     L = lib()
+    if key_type == "strings":
+        if isinstance(keys, tuple) and len(keys) == 2 and isinstance(keys[0], np.ndarray):
+            data, key_offsets = keys
+        else:
+            data, key_offsets = _strings_to_arrays(keys)
+        data = np.ascontiguousarray(data, dtype=np.uint8)
+        key_offsets = np.ascontiguousarray(key_offsets, dtype=np.uint64)
+        st = L.rsb_build_batch_strings(eng.handle, _ptr(data), _ptr(key_offsets), _ptr(offsets), nsets, bucket_size,
+                                       leaf_size, flags & RSB_ROTATE, outs, ctypes.byref(stats))
+        _check(st, "build_batch")
+        funcs = [GPURecSplit(bucket_size=bucket_size, leaf_size=leaf_size, rotate=rotate,
+                             _handle=ctypes.c_void_p(outs[i])) for i in range(nsets)]
+        return funcs, stats.as_dict()
     if keys_on_device:
         kp = ctypes.c_void_p(keys)
         if key_type is None:
@@ -359,6 +385,76 @@ def build_batch(keys: np.ndarray, set_offsets, bucket_size: int, leaf_size: int,
     funcs = [GPURecSplit(bucket_size=bucket_size, leaf_size=leaf_size, rotate=rotate, _handle=ctypes.c_void_p(outs[i]))
              for i in range(nsets)]
     return funcs, stats.as_dict()
+
+
+class Server:
+    """Continuous batching of build requests (rsb_server_*).
+
+    ``inflight`` workers, each with its own engine, take the oldest queued request plus
+    every queued request of the same (leaf size, bucket size, rotate, key kind) class while
+    the batch's estimated device working set fits ``hbm_budget / inflight`` bytes, and build
+    them as one batched pipeline. ``submit_*`` copies the keys and returns an id at once;
+    ``wait(id)`` returns (GPURecSplit, info dict) with the request's timestamps.
+    """
+
+    def __init__(self, hbm_budget: int, inflight: int = 2, max_batch_keys: int = 0, device: int = 0):
+        h = ctypes.c_void_p()
+        _check(lib().rsb_server_create(device, hbm_budget, inflight, max_batch_keys, ctypes.byref(h)),
+               "rsb_server_create")
+        self._h = h
+        self._params = {}
+
+    def submit_strings(self, keys, bucket_size: int, leaf_size: int, rotate: bool = True) -> int:
+        if isinstance(keys, tuple) and len(keys) == 2 and isinstance(keys[0], np.ndarray):
+            data, offsets = keys
+        else:
+            data, offsets = _strings_to_arrays(keys)
+        data = np.ascontiguousarray(data, dtype=np.uint8)
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+        rid = ctypes.c_uint64()
+        _check(lib().rsb_server_submit_strings(self._h, _ptr(data), _ptr(offsets), offsets.size - 1, bucket_size,
+                                               leaf_size, RSB_ROTATE if rotate else 0, ctypes.byref(rid)),
+               "rsb_server_submit_strings")
+        self._params[rid.value] = (bucket_size, leaf_size, rotate)
+        return rid.value
+
+    def submit_hash128(self, keys: np.ndarray, bucket_size: int, leaf_size: int, rotate: bool = True) -> int:
+        k = np.ascontiguousarray(keys, dtype=np.uint64).reshape(-1, 2)
+        rid = ctypes.c_uint64()
+        _check(lib().rsb_server_submit_hash128(self._h, _ptr(k), k.shape[0], bucket_size, leaf_size,
+                                               RSB_ROTATE if rotate else 0, ctypes.byref(rid)),
+               "rsb_server_submit_hash128")
+        self._params[rid.value] = (bucket_size, leaf_size, rotate)
+        return rid.value
+
+    def wait(self, rid: int, timeout_s: float = -1.0):
+        out = ctypes.c_void_p()
+        info = RequestInfo()
+        st = lib().rsb_server_wait(self._h, rid, timeout_s, ctypes.byref(out), ctypes.byref(info))
+        if st == 7:  # still running: the request stays queued
+            raise RSBError(st, "rsb_server_wait")
+        b, leaf, rot = self._params.pop(rid, (0, 0, True))
+        _check(st, "rsb_server_wait")
+        f = GPURecSplit(bucket_size=b, leaf_size=leaf, rotate=rot, _handle=out)
+        return f, {"submit_s": info.submit_s, "admit_s": info.admit_s, "done_s": info.done_s,
+                   "batch_requests": info.batch_requests, "batch_keys": info.batch_keys}
+
+    def close(self) -> None:
+        if self._h:
+            lib().rsb_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def hash_strings(keys, engine: Optional[Engine] = None) -> np.ndarray:
@@ -404,5 +500,5 @@ def hash_u64(keys: np.ndarray, engine: Optional[Engine] = None) -> np.ndarray:
     return out
 
 
-__all__ = ["GPURecSplit", "Engine", "RSBError", "lib", "build_library", "golomb_memo", "hash_strings", "hash_u64",
+__all__ = ["GPURecSplit", "Engine", "Server", "build_batch", "RSBError", "lib", "build_library", "golomb_memo", "hash_strings", "hash_u64",
            "default_engine", "LIB_PATH"]

@@ -866,6 +866,25 @@ rsb_status rsb_build_batch_u64(rsb_engine *e, const uint64_t *keys, const uint64
                               [=] { launch_hash_u64(dk, n, k128, st); });
 }
 
+rsb_status rsb_build_batch_strings(rsb_engine *e, const uint8_t *bytes, const uint64_t *offsets,
+                                   const uint64_t *set_offsets, uint32_t nsets, uint64_t bucket_size, uint32_t leaf,
+                                   uint32_t flags, rsb_mphf **outs, rsb_stats *stats) {
+    rsb_status s = check_batch(e, set_offsets, nsets, bucket_size, leaf, outs);
+    if (s != RSB_OK) return s;
+    if (!offsets) return RSB_ERR_BAD_ARG;
+    const uint64_t n = set_offsets[nsets];
+    const uint8_t *db;
+    const uint64_t *doff;
+    s = stage_strings(e, bytes, offsets, n, flags, &db, &doff);
+    if (s != RSB_OK) return s;
+    s = ensure(e->keys128, 2 * n);
+    if (s != RSB_OK) return s;
+    uint64_t *k128 = e->keys128.p;
+    cudaStream_t st = e->stream;
+    return build_batch_device(e, k128, set_offsets, nsets, bucket_size, leaf, flags, outs, stats,
+                              [=] { launch_hash_strings(db, doff, n, k128, st); });
+}
+
 rsb_status rsb_hash_strings(rsb_engine *e, const uint8_t *bytes, const uint64_t *offsets, uint64_t n, uint32_t flags,
                             rsb_hash128 *out) {
     if (!e || !offsets || !out) return RSB_ERR_BAD_ARG;

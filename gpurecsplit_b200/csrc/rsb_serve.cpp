@@ -1,0 +1,304 @@
+// Serving: continuous batching of build requests over several engines on one device.
+//
+// Each of `inflight` workers owns an engine (its own CUDA stream and cached scratch). A free
+// worker takes the oldest queued request plus every other queued request of the same class
+// (leaf size, bucket size, flags, key kind) in arrival order while their estimated device
+// working set fits its share of the HBM budget, builds them as one batch
+// (rsb_build_batch_*), and hands each request its own function. Requests that arrive while
+// batches run join the next batch a worker forms, and batches of different workers overlap
+// on the device. Each engine's cached scratch is bounded by the largest batch it ran, so
+// the server's device memory stays within the budget.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <new>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "rsb.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    uint64_t id = 0;
+    uint32_t leaf = 0, flags = 0;
+    uint64_t bucket = 0;
+    bool strings = false;
+    uint64_t n = 0;
+    std::vector<uint8_t> bytes;      // string keys, concatenated
+    std::vector<uint64_t> offsets;   // n + 1 entries into bytes
+    std::vector<rsb_hash128> keys;   // hash128 keys
+    uint64_t mem = 0;                // estimated device working set
+    double submit_s = 0, admit_s = 0, done_s = 0;
+    uint32_t batch_requests = 0;
+    uint64_t batch_keys = 0;
+    bool done = false;
+    rsb_status status = RSB_OK;
+    rsb_mphf *result = nullptr;
+
+    bool same_class(const Request &o) const {
+        return leaf == o.leaf && bucket == o.bucket && flags == o.flags && strings == o.strings;
+    }
+};
+
+// Device bytes of one build: hashes, partitioned keys, bucket ids, node arrays (< n nodes),
+// per-bucket arrays, encoder output, string staging; plus the engine's 1/8 regrowth headroom.
+uint64_t working_set(uint64_t n, uint64_t bucket, uint64_t string_bytes) {
+    const uint64_t per_key = 16 + 8 + 4 + 23 + 4 + 2 + (string_bytes ? 16 : 0);
+    const uint64_t per_bucket = 48;
+    const uint64_t nb = n / (bucket ? bucket : 1) + 1;
+    const uint64_t raw = n * per_key + nb * per_bucket + string_bytes + (4ull << 20);
+    return raw + raw / 8;
+}
+
+}  // namespace
+
+struct rsb_server {
+    int device = 0;
+    uint64_t budget = 0, share = 0, max_batch_keys = 0;
+    Clock::time_point t0;
+    std::vector<rsb_engine *> engines;
+    std::vector<std::thread> workers;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Request *> pending;
+    std::unordered_map<uint64_t, Request *> requests;
+    uint64_t next_id = 1;
+    bool stopping = false;
+
+    double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+};
+
+namespace {
+
+// Builds the requests of one batch; on a batch failure (e.g. a duplicate key in one
+// request) every request is built alone so that only the faulty one fails.
+void build(rsb_engine *e, std::vector<Request *> &batch) {
+    const uint32_t nsets = (uint32_t)batch.size();
+    const Request &r0 = *batch[0];
+    std::vector<uint64_t> set_offsets(nsets + 1, 0);
+    for (uint32_t s = 0; s < nsets; ++s) set_offsets[s + 1] = set_offsets[s] + batch[s]->n;
+    std::vector<rsb_mphf *> outs(nsets, nullptr);
+    rsb_status st;
+    if (r0.strings) {
+        std::vector<uint64_t> offsets(set_offsets[nsets] + 1, 0);
+        uint64_t total_bytes = 0;
+        for (auto *r : batch) total_bytes += r->bytes.size();
+        std::vector<uint8_t> bytes(total_bytes);
+        uint64_t k = 0, b = 0;
+        for (auto *r : batch) {
+            if (!r->bytes.empty()) std::memcpy(bytes.data() + b, r->bytes.data(), r->bytes.size());
+            for (uint64_t i = 0; i < r->n; ++i) offsets[k + i] = b + r->offsets[i];
+            k += r->n;
+            b += r->bytes.size();
+        }
+        offsets[k] = b;
+        st = rsb_build_batch_strings(e, bytes.data(), offsets.data(), set_offsets.data(), nsets, r0.bucket, r0.leaf,
+                                     r0.flags, outs.data(), nullptr);
+    } else {
+        std::vector<rsb_hash128> keys(set_offsets[nsets]);
+        uint64_t k = 0;
+        for (auto *r : batch) {
+            if (r->n) std::memcpy(keys.data() + k, r->keys.data(), r->n * sizeof(rsb_hash128));
+            k += r->n;
+        }
+        st = rsb_build_batch_hash128(e, keys.data(), set_offsets.data(), nsets, r0.bucket, r0.leaf, r0.flags,
+                                     outs.data(), nullptr);
+    }
+    if (st == RSB_OK) {
+        for (uint32_t s = 0; s < nsets; ++s) {
+            batch[s]->result = outs[s];
+            batch[s]->status = RSB_OK;
+        }
+        return;
+    }
+    if (nsets == 1) {
+        batch[0]->status = st;
+        return;
+    }
+    for (auto *r : batch) {
+        std::vector<Request *> one{r};
+        build(e, one);
+    }
+}
+
+void worker(rsb_server *S, size_t w) {
+    rsb_engine *e = S->engines[w];
+    for (;;) {
+        std::vector<Request *> batch;
+        uint64_t keys = 0;
+        {
+            std::unique_lock<std::mutex> lock(S->mu);
+            S->cv_work.wait(lock, [&] { return S->stopping || !S->pending.empty(); });
+            if (S->pending.empty()) return;  // stopping and drained
+            const Request first = *S->pending.front();
+            uint64_t mem = 0;
+            for (auto it = S->pending.begin(); it != S->pending.end();) {
+                Request *r = *it;
+                if (r->same_class(first) &&
+                    (batch.empty() || (mem + r->mem <= S->share && keys + r->n <= S->max_batch_keys))) {
+                    batch.push_back(r);
+                    mem += r->mem;
+                    keys += r->n;
+                    it = S->pending.erase(it);
+                } else {
+                    ++it;
+                }
+            }
+            const double t = S->now();
+            for (auto *r : batch) r->admit_s = t;
+        }
+        if (batch.size() == 1 && batch[0]->mem > S->share) {
+            batch[0]->status = RSB_ERR_OOM;  // larger than this worker's share of the budget
+        } else {
+            build(e, batch);
+        }
+        {
+            std::lock_guard<std::mutex> lock(S->mu);
+            const double t = S->now();
+            for (auto *r : batch) {
+                r->done = true;
+                r->done_s = t;
+                r->batch_requests = (uint32_t)batch.size();
+                r->batch_keys = keys;
+                r->bytes.clear();
+                r->bytes.shrink_to_fit();
+                r->offsets.clear();
+                r->offsets.shrink_to_fit();
+                r->keys.clear();
+                r->keys.shrink_to_fit();
+            }
+        }
+        S->cv_done.notify_all();
+    }
+}
+
+rsb_status enqueue(rsb_server *S, Request *r, uint64_t *id) {
+    {
+        std::lock_guard<std::mutex> lock(S->mu);
+        if (S->stopping) {
+            delete r;
+            return RSB_ERR_BAD_ARG;
+        }
+        r->id = S->next_id++;
+        r->submit_s = S->now();
+        S->pending.push_back(r);
+        S->requests[r->id] = r;
+        *id = r->id;
+    }
+    S->cv_work.notify_one();
+    return RSB_OK;
+}
+
+bool valid_params(uint64_t bucket, uint32_t leaf) { return bucket > 0 && leaf >= 2 && leaf <= 24; }
+
+}  // namespace
+
+extern "C" {
+
+rsb_status rsb_server_create(int device, uint64_t hbm_budget, uint32_t inflight, uint64_t max_batch_keys,
+                             rsb_server **out) {
+    if (!out || inflight == 0 || inflight > 16 || hbm_budget == 0) return RSB_ERR_BAD_ARG;
+    auto *S = new (std::nothrow) rsb_server;
+    if (!S) return RSB_ERR_OOM;
+    S->device = device;
+    S->budget = hbm_budget;
+    S->share = hbm_budget / inflight;
+    S->max_batch_keys = max_batch_keys ? max_batch_keys : (uint64_t)1 << 31;
+    S->t0 = Clock::now();
+    for (uint32_t i = 0; i < inflight; ++i) {
+        rsb_engine *e = nullptr;
+        const rsb_status st = rsb_engine_create(device, nullptr, &e);
+        if (st != RSB_OK) {
+            for (auto *x : S->engines) rsb_engine_destroy(x);
+            delete S;
+            return st;
+        }
+        S->engines.push_back(e);
+    }
+    for (size_t i = 0; i < S->engines.size(); ++i) S->workers.emplace_back(worker, S, i);
+    *out = S;
+    return RSB_OK;
+}
+
+rsb_status rsb_server_submit_strings(rsb_server *S, const uint8_t *bytes, const uint64_t *offsets, uint64_t n,
+                                     uint64_t bucket, uint32_t leaf, uint32_t flags, uint64_t *id) {
+    if (!S || !offsets || !id || !valid_params(bucket, leaf)) return RSB_ERR_BAD_ARG;
+    for (uint64_t i = 0; i < n; ++i)
+        if (offsets[i + 1] < offsets[i]) return RSB_ERR_BAD_ARG;
+    auto *r = new (std::nothrow) Request;
+    if (!r) return RSB_ERR_OOM;
+    r->strings = true;
+    r->leaf = leaf;
+    r->bucket = bucket;
+    r->flags = flags & RSB_ROTATE;
+    r->n = n;
+    const uint64_t b0 = offsets[0], b1 = offsets[n];
+    r->bytes.assign(bytes + b0, bytes + b1);
+    r->offsets.resize(n + 1);
+    for (uint64_t i = 0; i <= n; ++i) r->offsets[i] = offsets[i] - b0;
+    r->mem = working_set(n, bucket, b1 - b0);
+    return enqueue(S, r, id);
+}
+
+rsb_status rsb_server_submit_hash128(rsb_server *S, const rsb_hash128 *keys, uint64_t n, uint64_t bucket,
+                                     uint32_t leaf, uint32_t flags, uint64_t *id) {
+    if (!S || (n && !keys) || !id || !valid_params(bucket, leaf)) return RSB_ERR_BAD_ARG;
+    auto *r = new (std::nothrow) Request;
+    if (!r) return RSB_ERR_OOM;
+    r->leaf = leaf;
+    r->bucket = bucket;
+    r->flags = flags & RSB_ROTATE;
+    r->n = n;
+    r->keys.assign(keys, keys + n);
+    r->mem = working_set(n, bucket, 0);
+    return enqueue(S, r, id);
+}
+
+rsb_status rsb_server_wait(rsb_server *S, uint64_t id, double timeout_s, rsb_mphf **out, rsb_request_info *info) {
+    if (!S || !out) return RSB_ERR_BAD_ARG;
+    std::unique_lock<std::mutex> lock(S->mu);
+    auto it = S->requests.find(id);
+    if (it == S->requests.end()) return RSB_ERR_BAD_ARG;
+    Request *r = it->second;
+    auto ready = [&] { return r->done; };
+    if (timeout_s < 0) S->cv_done.wait(lock, ready);
+    else if (!S->cv_done.wait_for(lock, std::chrono::duration<double>(timeout_s), ready)) return RSB_ERR_TIMEOUT;
+    if (info) {
+        info->submit_s = r->submit_s;
+        info->admit_s = r->admit_s;
+        info->done_s = r->done_s;
+        info->batch_requests = r->batch_requests;
+        info->batch_keys = r->batch_keys;
+    }
+    const rsb_status st = r->status;
+    *out = r->result;
+    S->requests.erase(it);
+    delete r;
+    return st;
+}
+
+rsb_status rsb_server_destroy(rsb_server *S) {
+    if (!S) return RSB_ERR_BAD_ARG;
+    {
+        std::lock_guard<std::mutex> lock(S->mu);
+        S->stopping = true;
+    }
+    S->cv_work.notify_all();
+    for (auto &t : S->workers) t.join();
+    for (auto *e : S->engines) rsb_engine_destroy(e);
+    for (auto &kv : S->requests) {
+        if (kv.second->result) rsb_free(kv.second->result);
+        delete kv.second;
+    }
+    delete S;
+    return RSB_OK;
+}
+
+}  // extern "C"

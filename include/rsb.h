@@ -113,6 +113,38 @@ rsb_status rsb_build_batch_hash128(rsb_engine *engine, const rsb_hash128 *keys, 
 rsb_status rsb_build_batch_u64(rsb_engine *engine, const uint64_t *keys, const uint64_t *set_offsets, uint32_t nsets,
                                uint64_t bucket_size, uint32_t leaf_size, uint32_t flags, rsb_mphf **outs,
                                rsb_stats *stats);
+/* String keys: key i is bytes[offsets[i] .. offsets[i+1]) (offsets has set_offsets[nsets] + 1
+ * entries); set s is keys set_offsets[s] .. set_offsets[s+1]. */
+rsb_status rsb_build_batch_strings(rsb_engine *engine, const uint8_t *bytes, const uint64_t *offsets,
+                                   const uint64_t *set_offsets, uint32_t nsets, uint64_t bucket_size,
+                                   uint32_t leaf_size, uint32_t flags, rsb_mphf **outs, rsb_stats *stats);
+
+/* ---- serving: continuous batching of build requests (no reference counterpart) ---------
+ * A server owns `inflight` engines on one device, each with a worker thread. Submitted
+ * requests wait in a queue; whenever a worker is free it takes the oldest request and every
+ * other queued request of the same (leaf size, bucket size, flags) class, in arrival order,
+ * as long as their estimated device working set fits its share of `hbm_budget` bytes
+ * (hbm_budget / inflight), and builds them as one batch. Batches on different workers
+ * overlap on the device. A request that alone exceeds a worker's share fails with
+ * RSB_ERR_OOM. Results are bit-identical to plain builds of the same keys. */
+typedef struct rsb_server rsb_server;
+typedef struct rsb_request_info {
+    double submit_s, admit_s, done_s; /* steady-clock seconds since the server was created */
+    uint32_t batch_requests;          /* requests built together with this one (itself included) */
+    uint64_t batch_keys;
+} rsb_request_info;
+rsb_status rsb_server_create(int device, uint64_t hbm_budget, uint32_t inflight, uint64_t max_batch_keys,
+                             rsb_server **out);
+/* Copies the keys; returns at once with the request's id. */
+rsb_status rsb_server_submit_strings(rsb_server *server, const uint8_t *bytes, const uint64_t *offsets, uint64_t n,
+                                     uint64_t bucket_size, uint32_t leaf_size, uint32_t flags, uint64_t *id);
+rsb_status rsb_server_submit_hash128(rsb_server *server, const rsb_hash128 *keys, uint64_t n, uint64_t bucket_size,
+                                     uint32_t leaf_size, uint32_t flags, uint64_t *id);
+/* Waits for request `id` (at most timeout_s seconds; < 0 waits without limit) and hands
+ * over its function (the caller frees it with rsb_free). RSB_ERR_TIMEOUT if not done. */
+rsb_status rsb_server_wait(rsb_server *server, uint64_t id, double timeout_s, rsb_mphf **out, rsb_request_info *info);
+/* Stops accepting requests, finishes the queued ones and releases the engines. */
+rsb_status rsb_server_destroy(rsb_server *server);
 
 /* ---- queries and accessors --------------------------------------------------------- */
 

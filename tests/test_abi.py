@@ -69,3 +69,25 @@ def test_engine_without_device_fails_cleanly(rsb):
     with pytest.raises(rsb.RSBError) as e:
         rsb.Engine(0)
     assert e.value.name in ("NO_DEVICE", "CUDA")
+
+
+def test_server_argument_checks(rsb):
+    import ctypes
+    L = rsb.lib()
+    h = ctypes.c_void_p()
+    assert L.rsb_server_create(0, 1 << 30, 0, 0, ctypes.byref(h)) == 1  # no workers
+    assert L.rsb_server_create(0, 0, 1, 0, ctypes.byref(h)) == 1        # no budget
+    assert L.rsb_server_create(0, 1 << 30, 1, 0, None) == 1
+    rid = ctypes.c_uint64()
+    assert L.rsb_server_submit_hash128(None, None, 0, 100, 8, 1, ctypes.byref(rid)) == 1
+    assert L.rsb_server_wait(None, 1, 0.0, ctypes.byref(h), None) == 1
+    assert L.rsb_server_destroy(None) == 1
+
+
+def test_server_without_device_fails_cleanly(rsb):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(rsb.RSBError) as e:
+        rsb.Server(hbm_budget=1 << 30, inflight=2)
+    assert e.value.name in ("NO_DEVICE", "CUDA")
