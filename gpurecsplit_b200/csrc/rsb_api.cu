@@ -418,35 +418,9 @@ rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint
     return RSB_OK;
 }
 
-// Batched construction: nsets independent key sets (set s = keys [h_off[s], h_off[s+1]))
-// in one device pipeline. Sets share the global bucket space, so the tree, the stage lists
-// and every search kernel run once for all sets; bucket assignment and the encoders are
-// set-aware. outs[s] receives a host-side function identical to the plain build of set s.
-rsb_status build_batch_device(rsb_engine *e, const uint64_t *keys128, const uint64_t *h_off, uint32_t nsets,
-                              uint64_t bucket_size, uint32_t leaf, uint32_t flags, rsb_mphf **outs, rsb_stats *stats,
-                              const std::function<void()> &hash_keys) {
-    const bool rotate = (flags & RSB_ROTATE) != 0;
-    const LeafTables &lt = leaf_tables(leaf, rotate);
-    if (!shape_matches_kernels(lt.shape)) return RSB_ERR_INTERNAL;
-    DevTables tab;
-    rsb_status rs = get_device_tables(e, lt, leaf, rotate, tab);
-    if (rs != RSB_OK) return rs;
-    cudaStream_t st = e->stream;
-    const uint64_t n = h_off[nsets];
-    std::vector<uint64_t> set_nb(nsets);
-    uint64_t nb_total = 0, lower_cap = 0, cum_cap = 0, jump_cap = 0;
-    for (uint32_t s = 0; s < nsets; ++s) {
-        const uint64_t ns = h_off[s + 1] - h_off[s];
-        const uint64_t nb = std::max<uint64_t>(1, (ns + bucket_size - 1) / bucket_size);
-        set_nb[s] = nb;
-        nb_total += nb;
-        lower_cap += ((nb + 1) * 56 + 63) / 64 + 2;
-        cum_cap += (3 * (nb + 1) + 63) / 64 + 2;
-        jump_cap += jump_words_for(nb) + 2;
-    }
-    if (nb_total >= (1ull << 32) - 1) return RSB_ERR_BAD_ARG;
-    const uint64_t desc_cap = (8 * n) / 64 + 3 * (uint64_t)nsets + 16;
-    const uint64_t block_words = desc_cap + lower_cap + 2 * cum_cap + jump_cap;
+// Device scratch of a batched build of n keys in nsets sets and nb_total buckets whose
+// encoded output takes block_words words (also used to pre-size an engine).
+rsb_status ensure_batch_buffers(rsb_engine *e, uint64_t n, uint64_t nb_total, uint32_t nsets, uint64_t block_words) {
     const uint64_t max_nodes = n + 1;
     const uint32_t nslots = search_slots_needed(e->num_sms);
     RSB_ENSURE(e->sorted, n);
@@ -480,6 +454,42 @@ rsb_status build_batch_device(rsb_engine *e, const uint64_t *keys128, const uint
     RSB_ENSURE(e->ef_base, 4 * ((uint64_t)nsets + 1));
     RSB_ENSURE(e->set_ef, nsets);
     RSB_ENSURE(e->out_block, block_words);
+    return RSB_OK;
+}
+
+// Batched construction: nsets independent key sets (set s = keys [h_off[s], h_off[s+1]))
+// in one device pipeline. Sets share the global bucket space, so the tree, the stage lists
+// and every search kernel run once for all sets; bucket assignment and the encoders are
+// set-aware. outs[s] receives a host-side function identical to the plain build of set s.
+rsb_status build_batch_device(rsb_engine *e, const uint64_t *keys128, const uint64_t *h_off, uint32_t nsets,
+                              uint64_t bucket_size, uint32_t leaf, uint32_t flags, rsb_mphf **outs, rsb_stats *stats,
+                              const std::function<void()> &hash_keys) {
+    const bool rotate = (flags & RSB_ROTATE) != 0;
+    const LeafTables &lt = leaf_tables(leaf, rotate);
+    if (!shape_matches_kernels(lt.shape)) return RSB_ERR_INTERNAL;
+    DevTables tab;
+    rsb_status rs = get_device_tables(e, lt, leaf, rotate, tab);
+    if (rs != RSB_OK) return rs;
+    cudaStream_t st = e->stream;
+    const uint64_t n = h_off[nsets];
+    std::vector<uint64_t> set_nb(nsets);
+    uint64_t nb_total = 0, lower_cap = 0, cum_cap = 0, jump_cap = 0;
+    for (uint32_t s = 0; s < nsets; ++s) {
+        const uint64_t ns = h_off[s + 1] - h_off[s];
+        const uint64_t nb = std::max<uint64_t>(1, (ns + bucket_size - 1) / bucket_size);
+        set_nb[s] = nb;
+        nb_total += nb;
+        lower_cap += ((nb + 1) * 56 + 63) / 64 + 2;
+        cum_cap += (3 * (nb + 1) + 63) / 64 + 2;
+        jump_cap += jump_words_for(nb) + 2;
+    }
+    if (nb_total >= (1ull << 32) - 1) return RSB_ERR_BAD_ARG;
+    const uint64_t desc_cap = (8 * n) / 64 + 3 * (uint64_t)nsets + 16;
+    const uint64_t block_words = desc_cap + lower_cap + 2 * cum_cap + jump_cap;
+    rs = ensure_batch_buffers(e, n, nb_total, nsets, block_words);
+    if (rs != RSB_OK) return rs;
+    const uint64_t max_nodes = n + 1;
+    const uint32_t nslots = search_slots_needed(e->num_sms);
 
     NodeArrays nodes{e->nstart.p, e->nsize.p, e->nstage.p, e->seed.p, e->nwin.p};
     ScanTmp stmp{e->scan_tmp.p, e->scan_tmp.cap};
@@ -738,6 +748,23 @@ rsb_status rsb_engine_set_budget(rsb_engine *e, uint32_t shift, uint64_t min_can
     return RSB_OK;
 }
 
+rsb_status rsb_engine_reserve(rsb_engine *e, uint64_t keys, uint64_t bucket_size, uint64_t string_bytes,
+                              uint32_t sets) {
+    if (!e || bucket_size == 0 || sets == 0) return RSB_ERR_BAD_ARG;
+    RSB_CK(cudaSetDevice(e->device));
+    const uint64_t nb = keys / bucket_size + sets;
+    if (nb >= (1ull << 32) - 1) return RSB_ERR_BAD_ARG;
+    // Output block of the batched encoders: descriptors, EF lower bits, two upper-bit
+    // arrays and the jump table, with the per-set slack of build_batch_device.
+    const uint64_t block_words = (8 * keys) / 64 + 3 * (uint64_t)sets + 16 + ((nb + sets) * 56 + 63) / 64 +
+                                 2 * ((3 * (nb + sets) + 63) / 64) + jump_words_for(nb) + 24 * (uint64_t)sets;
+    rsb_status s = ensure_batch_buffers(e, keys, nb, sets, block_words);
+    if (s == RSB_OK) s = ensure(e->keys128, 2 * keys);
+    if (s == RSB_OK && string_bytes) s = ensure(e->bytes, string_bytes);
+    if (s == RSB_OK && string_bytes) s = ensure(e->offsets, keys + 1);
+    return s;
+}
+
 static rsb_status stage_keys128(rsb_engine *e, const rsb_hash128 *keys, uint64_t n, uint32_t flags, const uint64_t **dk) {
     if (flags & RSB_KEYS_ON_DEVICE) {
         *dk = (const uint64_t *)keys;
@@ -781,22 +808,27 @@ rsb_status rsb_build_u64(rsb_engine *e, const uint64_t *keys, uint64_t n, uint64
                         [=] { launch_hash_u64(dk, n, k128, st); });
 }
 
+// Host string keys: only the referenced bytes [offsets[0], offsets[n]) go to the device, and
+// the hash kernel subtracts offsets[0] (*base) from every offset.
 static rsb_status stage_strings(rsb_engine *e, const uint8_t *bytes, const uint64_t *offsets, uint64_t n, uint32_t flags,
-                                const uint8_t **db, const uint64_t **doff) {
+                                const uint8_t **db, const uint64_t **doff, uint64_t *base) {
     if (flags & RSB_KEYS_ON_DEVICE) {
         *db = bytes;
         *doff = offsets;
+        *base = 0;
         return RSB_OK;
     }
-    const uint64_t nbytes = offsets[n];
+    if (offsets[n] < offsets[0]) return RSB_ERR_BAD_ARG;
+    const uint64_t nbytes = offsets[n] - offsets[0];
     rsb_status s = ensure(e->bytes, nbytes);
     if (s != RSB_OK) return s;
     s = ensure(e->offsets, n + 1);
     if (s != RSB_OK) return s;
-    if (nbytes) RSB_CK(cudaMemcpyAsync(e->bytes.p, bytes, nbytes, cudaMemcpyHostToDevice, e->stream));
+    if (nbytes) RSB_CK(cudaMemcpyAsync(e->bytes.p, bytes + offsets[0], nbytes, cudaMemcpyHostToDevice, e->stream));
     RSB_CK(cudaMemcpyAsync(e->offsets.p, offsets, (n + 1) * 8, cudaMemcpyHostToDevice, e->stream));
     *db = e->bytes.p;
     *doff = e->offsets.p;
+    *base = offsets[0];
     return RSB_OK;
 }
 
@@ -807,14 +839,15 @@ rsb_status rsb_build_strings(rsb_engine *e, const uint8_t *bytes, const uint64_t
     if (!offsets) return RSB_ERR_BAD_ARG;
     const uint8_t *db;
     const uint64_t *doff;
-    s = stage_strings(e, bytes, offsets, n, flags, &db, &doff);
+    uint64_t sbase = 0;
+    s = stage_strings(e, bytes, offsets, n, flags, &db, &doff, &sbase);
     if (s != RSB_OK) return s;
     s = ensure(e->keys128, 2 * n);
     if (s != RSB_OK) return s;
     uint64_t *k128 = e->keys128.p;
     cudaStream_t st = e->stream;
     return build_device(e, k128, n, bucket_size, leaf, flags, out, (flags & kKeepSeeds) != 0,
-                        [=] { launch_hash_strings(db, doff, n, k128, st); });
+                        [=] { launch_hash_strings(db, doff, n, sbase, k128, st); });
 }
 
 static rsb_status check_batch(rsb_engine *e, const uint64_t *set_offsets, uint32_t nsets, uint64_t bucket_size,
@@ -875,14 +908,15 @@ rsb_status rsb_build_batch_strings(rsb_engine *e, const uint8_t *bytes, const ui
     const uint64_t n = set_offsets[nsets];
     const uint8_t *db;
     const uint64_t *doff;
-    s = stage_strings(e, bytes, offsets, n, flags, &db, &doff);
+    uint64_t sbase = 0;
+    s = stage_strings(e, bytes, offsets, n, flags, &db, &doff, &sbase);
     if (s != RSB_OK) return s;
     s = ensure(e->keys128, 2 * n);
     if (s != RSB_OK) return s;
     uint64_t *k128 = e->keys128.p;
     cudaStream_t st = e->stream;
     return build_batch_device(e, k128, set_offsets, nsets, bucket_size, leaf, flags, outs, stats,
-                              [=] { launch_hash_strings(db, doff, n, k128, st); });
+                              [=] { launch_hash_strings(db, doff, n, sbase, k128, st); });
 }
 
 rsb_status rsb_hash_strings(rsb_engine *e, const uint8_t *bytes, const uint64_t *offsets, uint64_t n, uint32_t flags,
@@ -891,11 +925,12 @@ rsb_status rsb_hash_strings(rsb_engine *e, const uint8_t *bytes, const uint64_t 
     RSB_CK(cudaSetDevice(e->device));
     const uint8_t *db;
     const uint64_t *doff;
-    rsb_status s = stage_strings(e, bytes, offsets, n, flags, &db, &doff);
+    uint64_t sbase = 0;
+    rsb_status s = stage_strings(e, bytes, offsets, n, flags, &db, &doff, &sbase);
     if (s != RSB_OK) return s;
     s = ensure(e->keys128, 2 * n);
     if (s != RSB_OK) return s;
-    launch_hash_strings(db, doff, n, e->keys128.p, e->stream);
+    launch_hash_strings(db, doff, n, sbase, e->keys128.p, e->stream);
     RSB_CK(cudaGetLastError());
     RSB_CK(cudaMemcpyAsync(out, e->keys128.p, n * 16, (flags & RSB_KEYS_ON_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                            e->stream));

@@ -26,7 +26,9 @@ void exclusive_scan_u32(const uint32_t *in, uint64_t *out, size_t n, ScanTmp tmp
 
 // ---- preparation (rsb_prep.cu) ----
 void launch_hash_u64(const uint64_t *keys, uint64_t n, uint64_t *out128, cudaStream_t st);
-void launch_hash_strings(const uint8_t *bytes, const uint64_t *offsets, uint64_t n, uint64_t *out128, cudaStream_t st);
+// Key i occupies bytes[offsets[i] - base, offsets[i + 1] - base).
+void launch_hash_strings(const uint8_t *bytes, const uint64_t *offsets, uint64_t n, uint64_t base, uint64_t *out128,
+                         cudaStream_t st);
 void launch_bucket_count(const uint64_t *keys128, uint64_t n, uint64_t nbuckets, uint32_t *counts, cudaStream_t st);
 void launch_bucket_check(const uint32_t *counts, uint64_t nbuckets, DevStatus *status, cudaStream_t st);
 void launch_bucket_scatter(const uint64_t *keys128, uint64_t n, uint64_t nbuckets, const uint64_t *acc,

@@ -135,12 +135,13 @@ __global__ void k_hash_u64(const uint64_t *__restrict__ keys, uint64_t n, ulongl
     }
 }
 
+// Key i is bytes[offsets[i] - base, offsets[i + 1] - base).
 __global__ void k_hash_strings(const uint8_t *__restrict__ bytes, const uint64_t *__restrict__ offsets, uint64_t n,
-                               ulonglong2 *__restrict__ out) {
+                               uint64_t base, ulonglong2 *__restrict__ out) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t b = offsets[i], e = offsets[i + 1];
         uint64_t h0 = 0, h1 = 0;
-        spooky128(bytes + b, e - b, h0, h1);
+        spooky128(bytes + (b - base), e - b, h0, h1);
         out[i] = make_ulonglong2(h1, h0);  // first = h1, second = h0 (util/Hash128.h:35)
     }
 }
@@ -348,8 +349,9 @@ void launch_hash_u64(const uint64_t *keys, uint64_t n, uint64_t *out128, cudaStr
     count_launches(1);
 }
 
-void launch_hash_strings(const uint8_t *bytes, const uint64_t *offsets, uint64_t n, uint64_t *out128, cudaStream_t st) {
-    k_hash_strings<<<grid_for(n, 128, 148 * 32), 128, 0, st>>>(bytes, offsets, n, (ulonglong2 *)out128);
+void launch_hash_strings(const uint8_t *bytes, const uint64_t *offsets, uint64_t n, uint64_t base, uint64_t *out128,
+                         cudaStream_t st) {
+    k_hash_strings<<<grid_for(n, 128, 148 * 32), 128, 0, st>>>(bytes, offsets, n, base, (ulonglong2 *)out128);
     count_launches(1);
 }
 

@@ -6,8 +6,12 @@
 // working set fits its share of the HBM budget, builds them as one batch
 // (rsb_build_batch_*), and hands each request its own function. Requests that arrive while
 // batches run join the next batch a worker forms, and batches of different workers overlap
-// on the device. Each engine's cached scratch is bounded by the largest batch it ran, so
-// the server's device memory stays within the budget.
+// on the device.
+//
+// Budget: at creation every engine reserves scratch for a fixed capacity (keys, string
+// bytes, buckets, sets) derived from its share, and a batch is admitted only while it fits
+// that capacity, so engines never grow and the server holds about hbm_budget bytes of
+// device memory from creation to destruction.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -34,7 +38,7 @@ struct Request {
     std::vector<uint8_t> bytes;      // string keys, concatenated
     std::vector<uint64_t> offsets;   // n + 1 entries into bytes
     std::vector<rsb_hash128> keys;   // hash128 keys
-    uint64_t mem = 0;                // estimated device working set
+    uint64_t buckets = 0;            // buckets of this request's function
     double submit_s = 0, admit_s = 0, done_s = 0;
     uint32_t batch_requests = 0;
     uint64_t batch_keys = 0;
@@ -47,14 +51,22 @@ struct Request {
     }
 };
 
-// Device bytes of one build: hashes, partitioned keys, bucket ids, node arrays (< n nodes),
-// per-bucket arrays, encoder output, string staging; plus the engine's 1/8 regrowth headroom.
-uint64_t working_set(uint64_t n, uint64_t bucket, uint64_t string_bytes) {
-    const uint64_t per_key = 16 + 8 + 4 + 23 + 4 + 2 + (string_bytes ? 16 : 0);
-    const uint64_t per_bucket = 48;
-    const uint64_t nb = n / (bucket ? bucket : 1) + 1;
-    const uint64_t raw = n * per_key + nb * per_bucket + string_bytes + (4ull << 20);
-    return raw + raw / 8;
+// Capacity of one worker with `share` bytes: a quarter for string bytes, the rest for keys
+// at ~62.5 device bytes each (hash 16, partitioned key 8, bucket id 4, node arrays 23,
+// descriptor 1, string offset 8, plus 40 per bucket at >= 16 keys per bucket), all with
+// the engine's 1/8 allocation headroom.
+struct Capacity {
+    uint64_t keys = 0, bytes = 0, buckets = 0;
+    uint32_t sets = 0;
+};
+
+Capacity capacity_for(uint64_t share) {
+    Capacity c;
+    c.bytes = (uint64_t)(share / 4 / 1.125);
+    c.keys = (uint64_t)(share * 0.75 / (1.125 * 62.5));
+    c.buckets = c.keys / 16 + 1024;
+    c.sets = 1u << 16;
+    return c;
 }
 
 }  // namespace
@@ -62,6 +74,7 @@ uint64_t working_set(uint64_t n, uint64_t bucket, uint64_t string_bytes) {
 struct rsb_server {
     int device = 0;
     uint64_t budget = 0, share = 0, max_batch_keys = 0;
+    Capacity cap;
     Clock::time_point t0;
     std::vector<rsb_engine *> engines;
     std::vector<std::thread> workers;
@@ -138,14 +151,18 @@ void worker(rsb_server *S, size_t w) {
             S->cv_work.wait(lock, [&] { return S->stopping || !S->pending.empty(); });
             if (S->pending.empty()) return;  // stopping and drained
             const Request first = *S->pending.front();
-            uint64_t mem = 0;
+            const Capacity &cap = S->cap;
+            uint64_t bytes = 0, buckets = 0;
             for (auto it = S->pending.begin(); it != S->pending.end();) {
                 Request *r = *it;
-                if (r->same_class(first) &&
-                    (batch.empty() || (mem + r->mem <= S->share && keys + r->n <= S->max_batch_keys))) {
+                const bool fits = keys + r->n <= cap.keys && bytes + r->bytes.size() <= cap.bytes &&
+                                  buckets + r->buckets <= cap.buckets && batch.size() < cap.sets &&
+                                  keys + r->n <= S->max_batch_keys;
+                if (r->same_class(first) && (batch.empty() || fits)) {
                     batch.push_back(r);
-                    mem += r->mem;
                     keys += r->n;
+                    bytes += r->bytes.size();
+                    buckets += r->buckets;
                     it = S->pending.erase(it);
                 } else {
                     ++it;
@@ -154,7 +171,9 @@ void worker(rsb_server *S, size_t w) {
             const double t = S->now();
             for (auto *r : batch) r->admit_s = t;
         }
-        if (batch.size() == 1 && batch[0]->mem > S->share) {
+        const Request &r0 = *batch[0];
+        if (batch.size() == 1 &&
+            (r0.n > S->cap.keys || r0.bytes.size() > S->cap.bytes || r0.buckets > S->cap.buckets)) {
             batch[0]->status = RSB_ERR_OOM;  // larger than this worker's share of the budget
         } else {
             build(e, batch);
@@ -211,10 +230,15 @@ rsb_status rsb_server_create(int device, uint64_t hbm_budget, uint32_t inflight,
     S->budget = hbm_budget;
     S->share = hbm_budget / inflight;
     S->max_batch_keys = max_batch_keys ? max_batch_keys : (uint64_t)1 << 31;
+    S->cap = capacity_for(S->share);
     S->t0 = Clock::now();
     for (uint32_t i = 0; i < inflight; ++i) {
         rsb_engine *e = nullptr;
-        const rsb_status st = rsb_engine_create(device, nullptr, &e);
+        rsb_status st = rsb_engine_create(device, nullptr, &e);
+        if (st == RSB_OK) {
+            st = rsb_engine_reserve(e, S->cap.keys, 16, S->cap.bytes, S->cap.sets);
+            if (st != RSB_OK) rsb_engine_destroy(e);
+        }
         if (st != RSB_OK) {
             for (auto *x : S->engines) rsb_engine_destroy(x);
             delete S;
@@ -243,7 +267,7 @@ rsb_status rsb_server_submit_strings(rsb_server *S, const uint8_t *bytes, const 
     r->bytes.assign(bytes + b0, bytes + b1);
     r->offsets.resize(n + 1);
     for (uint64_t i = 0; i <= n; ++i) r->offsets[i] = offsets[i] - b0;
-    r->mem = working_set(n, bucket, b1 - b0);
+    r->buckets = std::max<uint64_t>(1, (n + bucket - 1) / bucket);
     return enqueue(S, r, id);
 }
 
@@ -257,7 +281,7 @@ rsb_status rsb_server_submit_hash128(rsb_server *S, const rsb_hash128 *keys, uin
     r->flags = flags & RSB_ROTATE;
     r->n = n;
     r->keys.assign(keys, keys + n);
-    r->mem = working_set(n, bucket, 0);
+    r->buckets = std::max<uint64_t>(1, (n + bucket - 1) / bucket);
     return enqueue(S, r, id);
 }
 

@@ -84,7 +84,7 @@ extern "C" rsb_status rsb_hash_strings_static(const uint8_t *bytes, const uint64
     bool ok = true;
     if (nbytes) ok &= cudaMemcpyAsync(d_bytes, bytes, nbytes, cudaMemcpyHostToDevice, st) == cudaSuccess;
     ok &= cudaMemcpyAsync(d_offsets, offsets, (n + 1) * 8, cudaMemcpyHostToDevice, st) == cudaSuccess;
-    if (ok) launch_hash_strings(d_bytes, d_offsets, n, d_hashes, st);
+    if (ok) launch_hash_strings(d_bytes, d_offsets, n, 0, d_hashes, st);
     ok &= cudaGetLastError() == cudaSuccess;
     if (ok) ok &= cudaMemcpyAsync(out, d_hashes, n * 16, cudaMemcpyDeviceToHost, st) == cudaSuccess;
     ok &= cudaStreamSynchronize(st) == cudaSuccess;

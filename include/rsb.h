@@ -80,6 +80,13 @@ rsb_status rsb_engine_destroy(rsb_engine *engine);
 /* Candidate budget of every seed search: 2^(g(m) + shift) seeds, at least 2^16 (default
  * shift 10). Exceeding it ends the build with RSB_ERR_SEARCH_BUDGET instead of looping. */
 rsb_status rsb_engine_set_budget(rsb_engine *engine, uint32_t shift, uint64_t min_candidates);
+/* Pre-sizes the engine's cached device scratch (no reference counterpart) for builds, plain
+ * or batched, of up to `keys` keys in up to `sets` sets, with buckets of at least
+ * `bucket_size` keys and up to `string_bytes` bytes of host string keys, so that such builds
+ * allocate no scratch (growing scratch frees and reallocates, which waits for the device).
+ * Returns RSB_ERR_OOM, leaving the engine usable, if the device cannot hold it. */
+rsb_status rsb_engine_reserve(rsb_engine *engine, uint64_t keys, uint64_t bucket_size, uint64_t string_bytes,
+                              uint32_t sets);
 
 /* ---- construction ------------------------------------------------------------------ */
 
@@ -120,13 +127,16 @@ rsb_status rsb_build_batch_strings(rsb_engine *engine, const uint8_t *bytes, con
                                    uint32_t leaf_size, uint32_t flags, rsb_mphf **outs, rsb_stats *stats);
 
 /* ---- serving: continuous batching of build requests (no reference counterpart) ---------
- * A server owns `inflight` engines on one device, each with a worker thread. Submitted
- * requests wait in a queue; whenever a worker is free it takes the oldest request and every
- * other queued request of the same (leaf size, bucket size, flags) class, in arrival order,
- * as long as their estimated device working set fits its share of `hbm_budget` bytes
- * (hbm_budget / inflight), and builds them as one batch. Batches on different workers
- * overlap on the device. A request that alone exceeds a worker's share fails with
- * RSB_ERR_OOM. Results are bit-identical to plain builds of the same keys. */
+ * A server owns `inflight` engines on one device, each with a worker thread. At creation
+ * every engine reserves scratch for its share of `hbm_budget` bytes (hbm_budget / inflight):
+ * room for a fixed number of keys, string bytes and buckets. Submitted requests wait in a
+ * queue; whenever a worker is free it takes the oldest request and every other queued
+ * request of the same (leaf size, bucket size, flags, key kind) class, in arrival order, as
+ * long as the batch fits that reservation (and `max_batch_keys`, 0 = no limit), and builds
+ * them as one batch. Batches on different workers overlap on the device. A request that
+ * alone exceeds a worker's reservation fails with RSB_ERR_OOM; a request whose batch fails
+ * is rebuilt alone, so only a faulty request (e.g. duplicate keys) fails. Results are
+ * bit-identical to plain builds of the same keys. */
 typedef struct rsb_server rsb_server;
 typedef struct rsb_request_info {
     double submit_s, admit_s, done_s; /* steady-clock seconds since the server was created */

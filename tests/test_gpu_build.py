@@ -223,3 +223,20 @@ def test_golden_digest(rsb, oracle_mod, engine, name):
     assert len(blob) == g["bytes"]
     assert hashlib.sha256(blob).hexdigest() == g["sha256"]
     assert f.get_bits() == g["bits"]
+
+
+def test_string_keys_as_slice_of_larger_buffer(rsb, oracle_mod, engine):
+    """offsets[0] > 0: only bytes [offsets[0], offsets[n]) belong to the keys."""
+    data, offsets = oracle_mod.keygen_strings(77, 30_000)
+    lo, hi = 10_000, 25_000
+    sl = offsets[lo:hi + 1]
+    rebased = (data[int(sl[0]):int(sl[-1])].copy(), sl - sl[0])
+    a = rsb.GPURecSplit((data, sl), bucket_size=100, leaf_size=8, key_type="strings", engine=engine)
+    b = rsb.GPURecSplit(rebased, bucket_size=100, leaf_size=8, key_type="strings", engine=engine)
+    assert a.serialize() == b.serialize()
+    assert np.array_equal(rsb.hash_strings((data, sl), engine=engine), oracle_mod.hash_strings(*rebased))
+    funcs, _ = rsb.build_batch((data, sl), np.array([0, 5000, hi - lo], dtype=np.uint64), 100, 8,
+                               key_type="strings", engine=engine)
+    first = (rebased[0], rebased[1][:5001])
+    assert funcs[0].serialize() == rsb.GPURecSplit(first, bucket_size=100, leaf_size=8, key_type="strings",
+                                                   engine=engine).serialize()

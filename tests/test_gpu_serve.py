@@ -136,3 +136,37 @@ def test_serve_batch_strings_entry(rsb, oracle_mod, engine):
     for (d, o), f in zip(parts, funcs):
         plain = rsb.GPURecSplit((d, o), bucket_size=100, leaf_size=8, key_type="strings", engine=engine)
         assert f.serialize() == plain.serialize()
+
+
+def test_serve_holds_its_budget(rsb, oracle_mod):
+    import torch
+    torch.cuda.init()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    budget = 3 << 30
+    with rsb.Server(hbm_budget=budget, inflight=3) as srv:
+        free1, _ = torch.cuda.mem_get_info()
+        rng = np.random.default_rng(8)
+        ids = []
+        for i in range(24):
+            b, leaf = [(100, 8), (1000, 12), (2000, 16)][i % 3]
+            n = int(rng.integers(1000, 400_000 if leaf < 16 else 100_000))
+            ids.append(srv.submit_strings(_string_keys(rng, n), b, leaf))
+        for i in ids:
+            srv.wait(i)
+        free2, _ = torch.cuda.mem_get_info()
+    reserved = free0 - free1
+    assert reserved <= budget + (256 << 20), reserved     # reservation ~ budget (+ streams, tables)
+    assert free1 - free2 <= 64 << 20, free1 - free2        # serving allocates no more scratch
+
+
+def test_engine_reserve_then_build(rsb, oracle_mod):
+    eng = rsb.Engine(0)
+    eng.reserve(200_000, 100, 0, 4)
+    keys = oracle_mod.keygen_hash128(12, 150_000)
+    f = rsb.GPURecSplit(keys, bucket_size=100, leaf_size=8, engine=eng)
+    assert f.serialize() == oracle_mod.build_mphf(keys, 8, 100).bytes.tobytes()
+    with pytest.raises(rsb.RSBError) as e:
+        eng.reserve(10, 0)
+    assert e.value.name == "BAD_ARG"
+    eng.close()
