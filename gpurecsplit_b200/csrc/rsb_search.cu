@@ -53,35 +53,45 @@ __device__ __forceinline__ uint32_t shl_clamp(uint32_t a, uint32_t b) {
 // Low 16 bits of remix32(hi ^ lo) of a 64-bit candidate.
 __device__ __forceinline__ uint32_t hash16(uint64_t v) { return remix32(uint32_t(v >> 32) ^ uint32_t(v)) & 0xFFFFu; }
 
-// cnt[s] += #{keys k : hash16(k + bu + lane + 32 s) < thr} for s < S, where bu is the
-// warp-uniform window base. The 64-bit key + base sum is formed once per key; when its low
-// word cannot carry into the high word within the window (all but ~S*32 / 2^32 of the
-// keys), every candidate differs only in the low word, so the high word's share of
-// remix32's first xor-shift (H = hi ^ hi >> 16) is hoisted and each candidate costs a
-// 32-bit add. The compare is done on h16 << 16 = (z << 16) ^ (z & 0xFFFF0000).
-template <int S>
-__device__ __forceinline__ void threshold_counts(const uint64_t *sk, uint32_t m, uint64_t bu, uint32_t thr,
-                                                 uint32_t *cnt) {
+// acc[s] += sum over keys of the part index p(k, x) of candidate x = bu + lane + 32 s, where
+// bu is the warp-uniform window base. The 64-bit key + base sum is formed once per key.
+// When its low 16 bits cannot overflow within the window (all but ~S*32 / 2^16 of the
+// keys), every candidate differs from it only in bits 0..15, so remix32's first xor-shift
+// term (hi ^ hi >> 16 ^ lo >> 16) is one per-key constant K and a candidate costs a 32-bit
+// add and an xor before the two multiply rounds; other keys take the plain 64-bit form.
+// hash16 << 16 is formed as (z << 16) ^ (z & 0xFFFF0000). With b = hash16 << 16, the remap r =
+// (hash16 * m) >> 16 is umulhi(b, m) and the part index r / SPLIT is umulhi(r, magic) with
+// magic = ceil(2^32 / SPLIT), exact for r < 2^16; for a full node (m = fan * SPLIT) the part
+// index is umulhi(b, fan) directly. Both multiplies run on the FMA pipe, beside the ALU work
+// of the hash. An exactly balanced split has sum_j j * size_j, so this sum is a necessary
+// condition for success.
+template <int S, bool FULL>
+__device__ __forceinline__ void moment_sums(const uint64_t *sk, uint32_t m, uint64_t bu, uint32_t mult, uint32_t magic,
+                                            uint32_t *acc) {
+    constexpr uint32_t kSpan = 32u * S;
+    static_assert(kSpan <= 0x10000u, "window wider than the hoisting allows");
     const uint32_t lane = threadIdx.x & 31;
-    const uint32_t thr16 = thr << 16;
 #pragma unroll 4
     for (uint32_t i = 0; i < m; ++i) {
         const uint64_t tu = sk[i] + bu;
         const uint32_t lo0 = (uint32_t)tu, hi = (uint32_t)(tu >> 32);
-        if (lo0 > 0xFFFFFFFFu - 32u * S) {
+        if ((lo0 & 0xFFFFu) > 0x10000u - kSpan) {
 #pragma unroll
-            for (int s = 0; s < S; ++s) cnt[s] += hash16(tu + lane + 32u * s) < thr;
+            for (int s = 0; s < S; ++s) {
+                const uint32_t r = __umulhi(hash16(tu + lane + 32u * s) << 16, mult);
+                acc[s] += FULL ? r : __umulhi(r, magic);
+            }
         } else {
-            const uint32_t H = hi ^ (hi >> 16);
+            const uint32_t K = hi ^ (hi >> 16) ^ (lo0 >> 16);
             const uint32_t l0 = lo0 + lane;
 #pragma unroll
             for (int s = 0; s < S; ++s) {
-                const uint32_t lo = l0 + 32u * s;
-                uint32_t z = lo ^ (lo >> 16) ^ H;
+                uint32_t z = (l0 + 32u * s) ^ K;
                 z *= 0x85ebca6bu;
                 z ^= z >> 13;
                 z *= 0xc2b2ae35u;
-                cnt[s] += ((z << 16) ^ (z & 0xFFFF0000u)) < thr16;
+                const uint32_t r = __umulhi((z << 16) ^ (z & 0xFFFF0000u), mult);
+                acc[s] += FULL ? r : __umulhi(r, magic);
             }
         }
     }
@@ -203,14 +213,14 @@ __global__ void __launch_bounds__(kHigherThreads) k_search_higher(SearchCtx c, i
 // candidates that already fail — packed equality is exact equality.
 // ---------------------------------------------------------------------------------------
 //
-// Two-phase evaluation. A seed can only split a node exactly if the keys falling below the
-// part boundary j*SPLIT closest to m/2 number exactly j*SPLIT — a necessary condition that
-// costs one threshold compare per key (hash16 < ceil(j*SPLIT*2^16/m)) instead of a part
-// count. Phase A applies it to every seed of a window (4 per lane); the few survivors
-// (about 1/sqrt(2*pi*m*p*(1-p)) of them, 3-8 %) go to a per-warp queue in shared memory,
-// and phase B gives each lane one queued seed for the exact part count. A warp drains its
-// queue before it leaves a node, so every seed below the node's final best is still fully
-// checked and the minimum is unchanged.
+// Two-phase evaluation. A seed can only split a node exactly if the sum over its keys of
+// the part index equals sum_j j * size_j — a necessary condition that costs one or two
+// multiply-highs and an add per key (moment_sums) instead of a packed part count, and that
+// about 1 / (2.5 * sqrt(m * var(p))) of the seeds pass (1.9 % at m = 112, fanout 7).
+// Phase A applies it to every seed of a window (8 per lane); the survivors go to a per-warp
+// queue in shared memory, and phase B gives each lane one queued seed for the exact part
+// count. A warp drains its queue before it leaves a node, so every seed below the node's
+// final best is still fully checked and the minimum is unchanged.
 // ---------------------------------------------------------------------------------------
 constexpr int kAggrSeedsPerLane = 8;
 constexpr uint32_t kAggrWindow = 32 * kAggrSeedsPerLane;
@@ -298,7 +308,8 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
     const uint32_t base = c.stage_info[kNumStages + STAGE];
     const uint64_t seed = start_seed(C::SEED_INDEX);
     uint32_t rng = gw * 2654435761u + 12345u;
-    uint32_t node = kEmpty, m = 0, fan = 0, tlo = 0, thi = 0, thr = 0, cstar = 0, qn = 0;
+    constexpr uint32_t kMagic = (uint32_t)((0x100000000ull + C::SPLIT - 1) / C::SPLIT);  // ceil(2^32 / SPLIT)
+    uint32_t node = kEmpty, m = 0, fan = 0, tlo = 0, thi = 0, t1 = 0, qn = 0;
     bool owner = false, full = false;
     uint64_t budget = 0;
     for (;;) {
@@ -330,14 +341,9 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
                 if (j < 4) tlo |= t << (8 * j);
                 else thi |= t << (8 * (j - 4));
             }
-            // filter boundary: the part boundary j*SPLIT (1 <= j < fan) closest to m/2
-            uint32_t js = 1;
-            for (uint32_t j = 2; j < fan; ++j) {
-                const int dj = (int)(2 * j * C::SPLIT) - (int)m, db = (int)(2 * js * C::SPLIT) - (int)m;
-                if (abs(dj) < abs(db)) js = j;
-            }
-            cstar = js * C::SPLIT;
-            thr = (uint32_t)((((uint64_t)cstar << 16) + m - 1) / m);
+            // phase A target: sum_j j * size_j
+            t1 = 0;
+            for (uint32_t j = 1; j < fan; ++j) t1 += j * (j + 1 < fan ? C::SPLIT : m - (fan - 1) * C::SPLIT);
             budget = budget_for(c, m);
             qn = 0;
         }
@@ -356,14 +362,15 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
             node = kEmpty;
             continue;
         }
-        // phase A: threshold count for S seeds per lane (seeds x0 + lane + 32 s)
+        // phase A: part-index sums for S seeds per lane (seeds x0 + lane + 32 s)
         uint32_t cnt[S];
 #pragma unroll
         for (int s = 0; s < S; ++s) cnt[s] = 0;
-        threshold_counts<S>(sk, m, seed + x0, thr, cnt);
+        if (full) moment_sums<S, true>(sk, m, seed + x0, fan, 0u, cnt);
+        else moment_sums<S, false>(sk, m, seed + x0, m, kMagic, cnt);
 #pragma unroll
         for (int s = 0; s < S; ++s) {
-            const bool pass = cnt[s] == cstar;
+            const bool pass = cnt[s] == t1;
             const unsigned b = __ballot_sync(0xffffffffu, pass);
             if (pass) q[qn + __popc(b & below)] = x0 + lane + 32u * s;
             qn += __popc(b);
@@ -442,23 +449,24 @@ __device__ __forceinline__ uint32_t rotl_leaf(uint32_t v, uint32_t r) {
 }
 
 // Left masks of the S bases x0 + lane + 32 s of a rotation-leaf window (bu = SEED + x0*LEAF),
-// with the same hoisting of the key + base sum as threshold_counts.
+// with the same per-key hoisting as moment_sums (the window spans 32*S*LEAF seeds).
 template <int LEAF, int S>
 __device__ __forceinline__ void left_masks(const uint64_t *sk, uint32_t nl, uint64_t bu, uint32_t *ml) {
+    constexpr uint32_t kSpan = 32u * S * LEAF;
+    static_assert(kSpan <= 0x10000u, "window wider than the hoisting allows");
     const uint32_t lane = threadIdx.x & 31;
     for (uint32_t i = 0; i < nl; ++i) {
         const uint64_t tu = sk[i] + bu;
         const uint32_t lo0 = (uint32_t)tu, hi = (uint32_t)(tu >> 32);
-        if (lo0 > 0xFFFFFFFFu - 32u * S * LEAF) {
+        if ((lo0 & 0xFFFFu) > 0x10000u - kSpan) {
 #pragma unroll
             for (int s = 0; s < S; ++s) ml[s] |= 1u << remap16(tu + (lane + 32u * s) * LEAF, LEAF);
         } else {
-            const uint32_t H = hi ^ (hi >> 16);
+            const uint32_t K = hi ^ (hi >> 16) ^ (lo0 >> 16);
             const uint32_t l0 = lo0 + lane * LEAF;
 #pragma unroll
             for (int s = 0; s < S; ++s) {
-                const uint32_t lo = l0 + 32u * s * LEAF;
-                uint32_t z = lo ^ (lo >> 16) ^ H;
+                uint32_t z = (l0 + 32u * s * LEAF) ^ K;
                 z *= 0x85ebca6bu;
                 z ^= z >> 13;
                 z *= 0xc2b2ae35u;
@@ -737,10 +745,10 @@ void search_leaves(const SearchCtx &c, int stage, cudaStream_t st) {
 
 // ---- eval-rate probe ------------------------------------------------------------------
 // The cheapest complete candidate evaluation of any search (key + seed, remix32, 16-bit
-// threshold compare, count) in the exact form of the aggregation filter (threshold_counts:
-// keys broadcast from shared memory, 8 candidates per lane, unrolled key loop), run at full
-// occupancy with no scheduling, no queues and no reductions: the integer ceiling for
-// remixAndRemap32 evaluations on this device.
+// remap to a part index, sum) in the exact form of the aggregation filter (moment_sums on a
+// full node: keys broadcast from shared memory, 8 candidates per lane, unrolled key loop),
+// run at full occupancy with no scheduling, no queues and no reductions: the integer
+// ceiling for remixAndRemap32 evaluations on this device.
 namespace {
 constexpr int kProbeKeys = 128;
 constexpr int kProbeIters = 32;
@@ -754,7 +762,7 @@ __global__ void __launch_bounds__(kThreads) k_probe(unsigned long long *sink) {
     for (int s = 0; s < kProbeSeeds; ++s) cnt[s] = 0;
     uint64_t bu = start_seed(17) + (blockIdx.x * (uint64_t)kWarpsPerCta + (threadIdx.x >> 5)) * 32 * kProbeSeeds;
     for (int it = 0; it < kProbeIters; ++it) {
-        threshold_counts<kProbeSeeds>(sk, kProbeKeys, bu, 30001u, cnt);
+        moment_sums<kProbeSeeds, true>(sk, kProbeKeys, bu, 7u, 0u, cnt);
         bu += 1ull << 32;
     }
     uint32_t tot = 0;
