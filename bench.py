@@ -307,6 +307,8 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
             "stage_ms": {"partition": st["ms_partition"], "search": {str(i): round(v, 3) for i, v in
                                                                      enumerate(ms_search) if v > 0},
                          "encode": st["ms_encode"], "total": st["ms_total"]},
+            "stage_geval_s": {str(i): round(st["evals_stage"][i] / (v * 1e-3) / 1e9, 1)
+                              for i, v in enumerate(ms_search) if v > 0.05},
             "step_ms": [round(x, 3) for x in step_ms],
         }
         print(json.dumps(line), flush=True)

@@ -59,14 +59,14 @@ __device__ __forceinline__ uint32_t hash16(uint64_t v) { return remix32(uint32_t
 // keys), every candidate differs from it only in bits 0..15, so remix32's first xor-shift
 // term (hi ^ hi >> 16 ^ lo >> 16) is one per-key constant K and a candidate costs a 32-bit
 // add and an xor before the two multiply rounds; other keys take the plain 64-bit form.
-// hash16 << 16 is formed as (z << 16) ^ (z & 0xFFFF0000). With b = hash16 << 16, the remap r =
-// (hash16 * m) >> 16 is umulhi(b, m) and the part index r / SPLIT is umulhi(r, magic) with
-// magic = ceil(2^32 / SPLIT), exact for r < 2^16; for a full node (m = fan * SPLIT) the part
-// index is umulhi(b, fan) directly. Both multiplies run on the FMA pipe, beside the ALU work
-// of the hash. An exactly balanced split has sum_j j * size_j, so this sum is a necessary
-// condition for success.
+// hash16 << 16 is formed as (z << 16) ^ (z & 0xFFFF0000). With b = hash16 << 16, the part
+// index ((hash16 * m) >> 16) / SPLIT of a full node (m = fan * SPLIT) is umulhi(b, fan); for
+// any other node it is umulhi(b, mult) >> 28 with mult = ceil(m * 2^28 / SPLIT) (< 2^32 as
+// m < 16 * SPLIT; exact for every 16-bit hash, every leaf size and node size, checked
+// exhaustively). The multiply-high runs on the FMA pipe, beside the ALU work of the hash. An
+// exactly balanced split has sum_j j * size_j, so this sum is a necessary condition.
 template <int S, bool FULL>
-__device__ __forceinline__ void moment_sums(const uint64_t *sk, uint32_t m, uint64_t bu, uint32_t mult, uint32_t magic,
+__device__ __forceinline__ void moment_sums(const uint64_t *sk, uint32_t m, uint64_t bu, uint32_t mult,
                                             uint32_t *acc) {
     constexpr uint32_t kSpan = 32u * S;
     static_assert(kSpan <= 0x10000u, "window wider than the hoisting allows");
@@ -79,7 +79,7 @@ __device__ __forceinline__ void moment_sums(const uint64_t *sk, uint32_t m, uint
 #pragma unroll
             for (int s = 0; s < S; ++s) {
                 const uint32_t r = __umulhi(hash16(tu + lane + 32u * s) << 16, mult);
-                acc[s] += FULL ? r : __umulhi(r, magic);
+                acc[s] += FULL ? r : r >> 28;
             }
         } else {
             const uint32_t K = hi ^ (hi >> 16) ^ (lo0 >> 16);
@@ -91,7 +91,7 @@ __device__ __forceinline__ void moment_sums(const uint64_t *sk, uint32_t m, uint
                 z ^= z >> 13;
                 z *= 0xc2b2ae35u;
                 const uint32_t r = __umulhi((z << 16) ^ (z & 0xFFFF0000u), mult);
-                acc[s] += FULL ? r : __umulhi(r, magic);
+                acc[s] += FULL ? r : r >> 28;
             }
         }
     }
@@ -308,8 +308,7 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
     const uint32_t base = c.stage_info[kNumStages + STAGE];
     const uint64_t seed = start_seed(C::SEED_INDEX);
     uint32_t rng = gw * 2654435761u + 12345u;
-    constexpr uint32_t kMagic = (uint32_t)((0x100000000ull + C::SPLIT - 1) / C::SPLIT);  // ceil(2^32 / SPLIT)
-    uint32_t node = kEmpty, m = 0, fan = 0, tlo = 0, thi = 0, t1 = 0, qn = 0;
+    uint32_t node = kEmpty, m = 0, fan = 0, tlo = 0, thi = 0, t1 = 0, mult = 0, qn = 0;
     bool owner = false, full = false;
     uint64_t budget = 0;
     for (;;) {
@@ -341,7 +340,8 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
                 if (j < 4) tlo |= t << (8 * j);
                 else thi |= t << (8 * (j - 4));
             }
-            // phase A target: sum_j j * size_j
+            // phase A target: sum_j j * size_j; part-index multiplier of non-full nodes
+            mult = (uint32_t)((((uint64_t)m << 28) + C::SPLIT - 1) / C::SPLIT);
             t1 = 0;
             for (uint32_t j = 1; j < fan; ++j) t1 += j * (j + 1 < fan ? C::SPLIT : m - (fan - 1) * C::SPLIT);
             budget = budget_for(c, m);
@@ -366,8 +366,8 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
         uint32_t cnt[S];
 #pragma unroll
         for (int s = 0; s < S; ++s) cnt[s] = 0;
-        if (full) moment_sums<S, true>(sk, m, seed + x0, fan, 0u, cnt);
-        else moment_sums<S, false>(sk, m, seed + x0, m, kMagic, cnt);
+        if (full) moment_sums<S, true>(sk, m, seed + x0, fan, cnt);
+        else moment_sums<S, false>(sk, m, seed + x0, mult, cnt);
 #pragma unroll
         for (int s = 0; s < S; ++s) {
             const bool pass = cnt[s] == t1;
@@ -762,7 +762,7 @@ __global__ void __launch_bounds__(kThreads) k_probe(unsigned long long *sink) {
     for (int s = 0; s < kProbeSeeds; ++s) cnt[s] = 0;
     uint64_t bu = start_seed(17) + (blockIdx.x * (uint64_t)kWarpsPerCta + (threadIdx.x >> 5)) * 32 * kProbeSeeds;
     for (int it = 0; it < kProbeIters; ++it) {
-        moment_sums<kProbeSeeds, true>(sk, kProbeKeys, bu, 7u, 0u, cnt);
+        moment_sums<kProbeSeeds, true>(sk, kProbeKeys, bu, 7u, cnt);
         bu += 1ull << 32;
     }
     uint32_t tot = 0;
