@@ -49,7 +49,7 @@ BUCKET = 2000
 SEED = 42
 PUBLISHED_NS_PER_KEY = 1000.0  # GpuRecSplit, l=16 b=2000 n=5M: 1.0 us/object (README.md:18)
 GOLDEN = os.path.join(ROOT, "tests", "golden", "golden_builds.json")
-PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "traffic.json")
+PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "traffic_k_search_aggr_u64_n5M_l16_b2000.json")
 
 
 def splitmix64_keys(seed: int, n: int) -> np.ndarray:
