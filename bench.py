@@ -132,14 +132,20 @@ def cpu_sample(buckets: int, seed: int = SEED):
 
 
 def time_cpu_oracle(buckets: int, threads: int) -> dict:
+    """SIMDRecSplit restated (the oracle with AVX-512 search loops) when the CPU has AVX-512,
+    else the scalar oracle, on `buckets` buckets of the workload with `threads` threads."""
     import oracle
+    simd = oracle.simd_supported()
     keys, n = cpu_sample(buckets)
     t0 = time.perf_counter()
-    res = oracle.build_mphf(keys, LEAF, BUCKET, True, threads=threads)
+    res = oracle.build_mphf(keys, LEAF, BUCKET, True, threads=threads, simd=simd)
     dt = time.perf_counter() - t0
+    impl = ("SIMDRecSplit restated: oracle with AVX-512 search loops (16 seeds per 512-bit vector)" if simd
+            else "scalar oracle (this CPU lacks AVX-512)")
     return {"value": dt * 1e9 / n, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{buckets} buckets of b={BUCKET} ({n} keys, same key stream and l={LEAF}) out of the "
-                      f"{(N_KEYS + BUCKET - 1) // BUCKET}-bucket workload; scalar oracle, {threads} threads",
+                      f"{(N_KEYS + BUCKET - 1) // BUCKET}-bucket workload; {impl}, {threads} threads on "
+                      f"{oracle.cpu_model()}",
             "seconds": dt, "bits_per_key": oracle.get_bits(res.bytes) / n}
 
 
@@ -149,6 +155,8 @@ def run_reference(args, rank: int, world: int) -> None:
     import oracle
     oracle.build()
     threads = os.cpu_count() or 1
+    if args.ref_buckets is None:
+        args.ref_buckets = 96 if oracle.simd_supported() else 24
     for _ in range(args.warmup):
         time_cpu_oracle(args.ref_buckets, threads)
     vals = [time_cpu_oracle(args.ref_buckets, threads) for _ in range(args.steps)]
@@ -161,8 +169,9 @@ def run_reference(args, rank: int, world: int) -> None:
         "config": workload_config(N_KEYS, world) | {"cpu_sample_buckets": args.ref_buckets},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": vals[0]["sample"]},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "CPU oracle (scalar restatement of SIMDRecSplit); the reference itself cannot be built here "
-                "(its sux, vectorclass, gcem, ips2ra and SpookyV2 submodules are empty)",
+        "note": "SIMDRecSplit restated on the host cores (the oracle with AVX-512 search loops, or the scalar "
+                "oracle on CPUs without AVX-512); the reference itself cannot be built here (its sux, "
+                "vectorclass, gcem, ips2ra and SpookyV2 submodules are empty)",
     }
     print(json.dumps(line), flush=True)
 
@@ -287,6 +296,8 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         if world == 1 and not args.no_cpu_baseline:
             import oracle
             oracle.build()
+            if args.cpu_buckets is None:
+                args.cpu_buckets = 192 if oracle.simd_supported() else 48
             cpu = time_cpu_oracle(args.cpu_buckets, os.cpu_count() or 1)
             cpu.pop("seconds", None)
         line = {
@@ -530,8 +541,8 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="rsb", choices=["rsb", "reference"])
     ap.add_argument("--n", type=int, default=N_KEYS)
-    ap.add_argument("--cpu-buckets", type=int, default=48)
-    ap.add_argument("--ref-buckets", type=int, default=24)
+    ap.add_argument("--cpu-buckets", type=int, default=None, help="CPU baseline sample (default 192, 48 without AVX-512)")
+    ap.add_argument("--ref-buckets", type=int, default=None, help="reference-arm sample (default 96, 24 without AVX-512)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", default="plain", choices=["plain", "batch", "serve"])
     ap.add_argument("--sets", type=int, default=1000)

@@ -16,7 +16,12 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+# Same source with the seed searches in AVX-512 intrinsics (SIMDRecSplit's lane layout):
+# the timed CPU baseline only. Loaded on request and only on CPUs that have the features.
+_SIMD_LIB_PATH = os.path.join(_HERE, "_build", "libsimdrs.so")
+_SIMD_FLAGS = ("avx512f", "avx512dq", "avx512bw", "avx512vl", "avx512_vpopcntdq")
 _lib = None
+_simd_lib = None
 
 STATUS = {0: "OK", 1: "BAD_ARG", 2: "DUPLICATE_KEY", 3: "BUCKET_TOO_LARGE", 4: "FORMAT"}
 
@@ -27,39 +32,78 @@ def build() -> str:
     return _LIB_PATH
 
 
+def simd_supported() -> bool:
+    """True when this CPU has the AVX-512 features libsimdrs.so is compiled for."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    flags = set(line.split(":", 1)[1].split())
+                    return all(x in flags for x in _SIMD_FLAGS)
+    except OSError:
+        pass
+    return False
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def simd_lib():
+    """The AVX-512 build (raises if this CPU lacks the features)."""
+    global _simd_lib
+    if _simd_lib is None:
+        if not simd_supported():
+            raise RuntimeError("this CPU lacks AVX-512 F/DQ/BW/VL/VPOPCNTDQ")
+        if not os.path.exists(_SIMD_LIB_PATH):
+            build()
+        _simd_lib = _configure(ctypes.CDLL(_SIMD_LIB_PATH))
+    return _simd_lib
+
+
 def lib():
     global _lib
     if _lib is None:
         if not os.path.exists(_LIB_PATH):
             build()
-        L = ctypes.CDLL(_LIB_PATH)
-        u64p = ctypes.POINTER(ctypes.c_uint64)
-        L.orc_memo.argtypes = [ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
-        L.orc_build.restype = ctypes.c_void_p
-        L.orc_build.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64,
-                                ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
-        L.orc_build_buckets.restype = ctypes.c_void_p
-        L.orc_build_buckets.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64,
-                                        ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64,
-                                        ctypes.POINTER(ctypes.c_int)]
-        L.orc_result_len.restype = ctypes.c_uint64
-        L.orc_result_len.argtypes = [ctypes.c_void_p, ctypes.c_int]
-        L.orc_result_copy.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
-        L.orc_free.argtypes = [ctypes.c_void_p]
-        L.orc_query.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p,
-                                ctypes.c_uint64, ctypes.c_void_p]
-        L.orc_get_bits.restype = ctypes.c_uint64
-        L.orc_get_bits.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64]
-        L.orc_keygen_hash128.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p]
-        L.orc_keygen_u64.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p]
-        L.orc_hash_u64.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]
-        L.orc_keygen_strings.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
-                                         ctypes.c_void_p, ctypes.c_void_p]
-        L.orc_hash_strings.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]
-        L.orc_remap16.restype = ctypes.c_uint32
-        L.orc_remap16.argtypes = [ctypes.c_uint64, ctypes.c_uint32]
-        _lib = L
+        _lib = _configure(ctypes.CDLL(_LIB_PATH))
     return _lib
+
+
+def _configure(L):
+    u64p = ctypes.POINTER(ctypes.c_uint64)
+    L.orc_memo.argtypes = [ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.orc_build.restype = ctypes.c_void_p
+    L.orc_build.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64,
+                            ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    L.orc_build_buckets.restype = ctypes.c_void_p
+    L.orc_build_buckets.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64,
+                                    ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64,
+                                    ctypes.POINTER(ctypes.c_int)]
+    L.orc_result_len.restype = ctypes.c_uint64
+    L.orc_result_len.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.orc_result_copy.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+    L.orc_free.argtypes = [ctypes.c_void_p]
+    L.orc_query.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p,
+                            ctypes.c_uint64, ctypes.c_void_p]
+    L.orc_get_bits.restype = ctypes.c_uint64
+    L.orc_get_bits.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64]
+    L.orc_keygen_hash128.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p]
+    L.orc_keygen_u64.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p]
+    L.orc_hash_u64.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]
+    L.orc_keygen_strings.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
+                                     ctypes.c_void_p, ctypes.c_void_p]
+    L.orc_hash_strings.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]
+    L.orc_remap16.restype = ctypes.c_uint32
+    L.orc_remap16.argtypes = [ctypes.c_uint64, ctypes.c_uint32]
+    return L
 
 
 def _ptr(a: np.ndarray):
@@ -84,19 +128,18 @@ def memo(leaf: int):
 class Build:
     """Result of one oracle build: serialized bytes, DFS seeds, node sizes, EF inputs."""
 
-    def __init__(self, handle):
-        L = lib()
-        self.bytes = self._get(handle, 0, np.uint8)
-        self.seeds = self._get(handle, 1, np.uint64)
-        self.sizes = self._get(handle, 2, np.uint32)
-        self.bucket_size_acc = self._get(handle, 3, np.uint64)
-        self.bucket_pos_acc = self._get(handle, 4, np.uint64)
-        self.evals_alg = int(self._get(handle, 5, np.uint64)[0])
+    def __init__(self, handle, L=None):
+        L = L or lib()
+        self.bytes = self._get(L, handle, 0, np.uint8)
+        self.seeds = self._get(L, handle, 1, np.uint64)
+        self.sizes = self._get(L, handle, 2, np.uint32)
+        self.bucket_size_acc = self._get(L, handle, 3, np.uint64)
+        self.bucket_pos_acc = self._get(L, handle, 4, np.uint64)
+        self.evals_alg = int(self._get(L, handle, 5, np.uint64)[0])
         L.orc_free(handle)
 
     @staticmethod
-    def _get(handle, which, dtype):
-        L = lib()
+    def _get(L, handle, which, dtype):
         n = L.orc_result_len(handle, which)
         a = np.zeros(n, dtype=dtype)
         if n:
@@ -104,15 +147,18 @@ class Build:
         return a
 
 
-def build_mphf(keys128: np.ndarray, leaf: int, bucket_size: int, rotate: bool = True, threads: int = 0) -> Build:
-    """keys128: uint64 array of shape (n, 2) holding (first, second)."""
+def build_mphf(keys128: np.ndarray, leaf: int, bucket_size: int, rotate: bool = True, threads: int = 0,
+               simd: bool = False) -> Build:
+    """keys128: uint64 array of shape (n, 2) holding (first, second). ``simd`` selects the
+    AVX-512 build of the searches (same output; the timed CPU baseline)."""
     keys128 = np.ascontiguousarray(keys128, dtype=np.uint64).reshape(-1, 2)
     threads = threads or os.cpu_count() or 1
+    L = simd_lib() if simd else lib()
     st = ctypes.c_int(0)
-    h = lib().orc_build(_ptr(keys128), keys128.shape[0], leaf, bucket_size, int(rotate), threads, ctypes.byref(st))
+    h = L.orc_build(_ptr(keys128), keys128.shape[0], leaf, bucket_size, int(rotate), threads, ctypes.byref(st))
     if not h:
         raise OracleError(st.value)
-    return Build(h)
+    return Build(h, L)
 
 
 def bucket_seeds(keys128: np.ndarray, leaf: int, bucket_size: int, buckets, rotate: bool = True,

@@ -26,6 +26,9 @@
 #include <mutex>
 #include <thread>
 #include <vector>
+#ifdef ORC_SIMD
+#include <immintrin.h>
+#endif
 
 namespace orc {
 
@@ -151,6 +154,9 @@ struct Stats {
 // Early exits below only prune failing candidates; they never change the minimum.
 // ---------------------------------------------------------------------------------------
 
+#ifndef ORC_SIMD
+namespace scalar {
+
 // higherLevel, SIMDRecSplit.hpp:250-317: exactly `split` keys must remap below `split`.
 static uint64_t search_higher(const uint64_t *keys, uint32_t m, uint32_t split, uint64_t seed) {
     for (uint64_t x = 0;; ++x) {
@@ -244,6 +250,13 @@ static uint64_t search_leaf_rotate(const uint64_t *keys, uint32_t leaf, uint64_t
     }
 }
 
+}  // namespace scalar
+namespace search = scalar;
+#else
+#include "simd_search.inc"
+namespace search = simd;
+#endif
+
 // ---------------------------------------------------------------------------------------
 // recSplit DFS, SIMDRecSplit.hpp:624-693. Seeds are recorded in DFS pre-order together
 // with their node sizes; children are partitioned stably by part as in :288-306, :395-412.
@@ -265,10 +278,10 @@ static void leaf_level(const Ctx &c, uint64_t *keys, uint32_t m, BucketOut &out,
     const uint64_t seed = kStartSeed[kNumStartSeeds - 1];
     uint64_t x;
     if (c.rotate && m == c.shape.leaf) {
-        x = search_leaf_rotate(keys, m, seed);
+        x = search::search_leaf_rotate(keys, m, seed);
         add_stat(st, x / m + 1, m);
     } else {
-        x = search_leaf_bruteforce(keys, m, seed);
+        x = search::search_leaf_bruteforce(keys, m, seed);
         add_stat(st, x + 1, m);
     }
     out.seeds.push_back(x);
@@ -284,7 +297,7 @@ static void rec_split(const Ctx &c, uint64_t *keys, uint64_t *tmp, uint32_t m, i
     if (m > s.upper) {  // fanout 2, SIMDRecSplit.hpp:631-635
         const uint32_t split = (uint16_t(m / 2 + s.upper - 1) / s.upper) * s.upper;
         const uint64_t seed = kStartSeed[level];
-        const uint64_t x = search_higher(keys, m, split, seed);
+        const uint64_t x = search::search_higher(keys, m, split, seed);
         add_stat(st, x + 1, m);
         out.seeds.push_back(x);
         out.sizes.push_back(m);
@@ -298,7 +311,7 @@ static void rec_split(const Ctx &c, uint64_t *keys, uint64_t *tmp, uint32_t m, i
     const bool upper_level = m > s.lower;  // :640 (second aggregation level) vs :651
     const uint32_t split = upper_level ? s.lower : s.leaf;
     const uint64_t seed = kStartSeed[kNumStartSeeds - (upper_level ? 3 : 2)];
-    const uint64_t x = search_aggr(keys, m, split, seed);
+    const uint64_t x = search::search_aggr(keys, m, split, seed);
     add_stat(st, x + 1, m);
     out.seeds.push_back(x);
     out.sizes.push_back(m);

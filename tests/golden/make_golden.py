@@ -5,7 +5,11 @@ rotation) and the SHA-256 of the oracle's serialized function for it. The GPU te
 the same workload on the device and compare digests, which checks full-size builds
 bit for bit without running the scalar oracle on the GPU box.
 
-    python tests/golden/make_golden.py [name ...]      # default: every missing entry
+    python tests/golden/make_golden.py [--simd] [name ...]   # default: every missing entry
+
+--simd builds with the oracle's AVX-512 search loops (oracle/_build/libsimdrs.so), which
+tests/test_oracle.py checks byte for byte against the scalar oracle; the entry records which
+build produced it. It is used for workloads the scalar build needs hours for (l = 24).
 """
 import hashlib
 import json
@@ -43,20 +47,23 @@ def keys_for(kind, seed, n):
     raise ValueError(kind)
 
 
-def main(names):
+def main(args):
+    simd = "--simd" in args
+    names = [a for a in args if a != "--simd"]
     db = json.load(open(OUT)) if os.path.exists(OUT) else {}
     todo = names or [k for k in WORKLOADS if k not in db]
     for name in todo:
         kind, seed, n, leaf, b, rot = WORKLOADS[name]
         t = time.time()
         keys = keys_for(kind, seed, n)
-        res = oracle.build_mphf(keys, leaf, b, rot)
+        res = oracle.build_mphf(keys, leaf, b, rot, simd=simd)
         dt = time.time() - t
         db[name] = {
             "kind": kind, "seed": seed, "n": n, "leaf": leaf, "bucket": b, "rotate": rot,
             "sha256": hashlib.sha256(res.bytes.tobytes()).hexdigest(), "bytes": int(res.bytes.size),
             "bits": oracle.get_bits(res.bytes), "nodes": int(res.seeds.size), "evals_alg": res.evals_alg,
             "oracle_seconds": round(dt, 1), "oracle_threads": os.cpu_count(),
+            "oracle_build": "avx512 search loops" if simd else "scalar",
         }
         print(name, db[name], flush=True)
         cur = json.load(open(OUT)) if os.path.exists(OUT) else {}

@@ -109,3 +109,19 @@ def test_oracle_u64_mixer_distinct_seconds(oracle_mod):
     k = oracle_mod.keygen_u64(42, 100000)
     h = oracle_mod.hash_u64(k)
     assert np.unique(h[:, 1]).size == k.size
+
+
+_SIMD_GRID = [(leaf, b, n, rot) for leaf in (2, 3, 5, 8, 11, 12, 16, 20, 24) for (b, n) in ((7, 500), (100, 3000), (2000, 2500))
+              for rot in (True, False) if not (leaf >= 20 and n > 600) and not (not rot and leaf >= 16 and n > 600)]
+
+
+@pytest.mark.parametrize("leaf,b,n,rot", _SIMD_GRID)
+def test_simd_oracle_equals_scalar(oracle_mod, leaf, b, n, rot):
+    """The AVX-512 search loops (the timed CPU baseline) give the scalar oracle's bytes."""
+    if not oracle_mod.simd_supported():
+        pytest.skip("CPU lacks AVX-512 F/DQ/BW/VL/VPOPCNTDQ")
+    keys = oracle_mod.keygen_hash128(leaf * 1000 + b + n, n)
+    a = oracle_mod.build_mphf(keys, leaf, b, rot, threads=4)
+    s = oracle_mod.build_mphf(keys, leaf, b, rot, threads=4, simd=True)
+    assert a.bytes.tobytes() == s.bytes.tobytes()
+    assert np.array_equal(a.seeds, s.seeds)
