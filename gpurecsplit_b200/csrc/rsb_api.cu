@@ -335,7 +335,7 @@ rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint
     launch_bucket_check(e->counts.p, nb, e->status.p, st);
     exclusive_scan_u32(e->counts.p, e->acc.p, nb, stmp, st);
     launch_bucket_scatter(keys128, n, nb, e->acc.p, e->counts.p, e->sorted.p, st);
-    launch_bucket_sort(e->sorted.p, e->acc.p, nb, e->status.p, st);
+    launch_bucket_dupcheck(e->sorted.p, e->acc.p, nb, e->status.p, st);
     // ---- tree ----
     launch_bucket_nodes(e->acc.p, nb, tab, e->node_count.p, st);
     exclusive_scan_u32(e->node_count.p, e->node_base.p, nb, stmp, st);
@@ -512,8 +512,9 @@ rsb_status build_batch_device(rsb_engine *e, const uint64_t *keys128, const uint
     launch_set_bucket_ids(keys128, n, e->set_key.p, e->set_bucket.p, nsets, nb_total, e->bucket_id.p, e->counts.p, st);
     launch_bucket_check(e->counts.p, nb_total, e->status.p, st);
     exclusive_scan_u32(e->counts.p, e->acc.p, nb_total, stmp, st);
-    launch_set_scatter(keys128, n, e->bucket_id.p, e->acc.p, e->counts.p, nb_total, e->sorted.p, st);
-    launch_bucket_sort(e->sorted.p, e->acc.p, nb_total, e->status.p, st);
+    launch_set_scatter(keys128, n, e->set_key.p, e->set_bucket.p, nsets, e->bucket_id.p, e->acc.p, e->counts.p, nb_total,
+                       e->sorted.p, st);
+    launch_bucket_dupcheck(e->sorted.p, e->acc.p, nb_total, e->status.p, st);
     // ---- tree ----
     launch_bucket_nodes(e->acc.p, nb_total, tab, e->node_count.p, st);
     exclusive_scan_u32(e->node_count.p, e->node_base.p, nb_total, stmp, st);

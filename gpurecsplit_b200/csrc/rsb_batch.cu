@@ -8,6 +8,7 @@
 // gets its own Golomb-Rice stream (starting at bit 0 of its own word vector, sentinel after
 // its last bucket) and its own double Elias-Fano index, exactly as its plain build would.
 #include "rsb_kernels.cuh"
+#include "rsb_partition.cuh"
 
 namespace rsb {
 
@@ -42,23 +43,43 @@ __global__ void k_set_nbuckets(const uint64_t *set_key, uint32_t nsets, uint64_t
     }
 }
 
-__global__ void k_set_bucket_ids(const ulonglong2 *__restrict__ keys, uint64_t n, const uint64_t *set_key,
-                                 const uint64_t *set_bucket, uint32_t nsets, uint32_t *bucket_id, uint32_t *counts) {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        // sets may be empty: take the last set whose first key is <= i
-        const uint32_t s = upper_index(set_key, nsets, i);
-        const uint64_t nb = set_bucket[s + 1] - set_bucket[s];
-        const uint32_t b = (uint32_t)(set_bucket[s] + remap128(keys[i].x, nb));
-        bucket_id[i] = b;
-        atomicAdd(&counts[b], 1u);
-    }
-}
-
-__global__ void k_set_scatter(const ulonglong2 *__restrict__ keys, uint64_t n, const uint32_t *bucket_id,
-                              const uint64_t *acc, uint32_t *cursor, uint64_t *sorted) {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t b = bucket_id[i];
-        sorted[acc[b] + atomicAdd(&cursor[b], 1u)] = keys[i].y;
+// Bucket ids of a batched build, counted per bucket. Keys are taken in contiguous chunks of
+// kPartChunk per CTA, so a chunk spans few sets: its set range is found once, each key
+// searches only inside it, and when the chunk's buckets fit kPartBins the counts are
+// gathered in shared memory and flushed with one global atomic per non-empty bucket.
+__global__ void __launch_bounds__(kPartThreads) k_set_bucket_ids(const ulonglong2 *__restrict__ keys, uint64_t n,
+                                                                  const uint64_t *set_key, const uint64_t *set_bucket,
+                                                                  uint32_t nsets, uint32_t *bucket_id, uint32_t *counts) {
+    __shared__ uint32_t bins[kPartBins];
+    __shared__ uint32_t s_lo, s_hi;
+    for (uint64_t c0 = (uint64_t)blockIdx.x * kPartChunk; c0 < n; c0 += (uint64_t)gridDim.x * kPartChunk) {
+        const uint64_t c1 = c0 + kPartChunk < n ? c0 + kPartChunk : n;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            // sets may be empty: a key belongs to the last set whose first key is <= it
+            s_lo = upper_index(set_key, nsets, c0);
+            s_hi = upper_index(set_key, nsets, c1 - 1);
+        }
+        __syncthreads();
+        const uint32_t lo = s_lo, hi = s_hi;
+        const uint64_t b0 = set_bucket[lo], nbins = set_bucket[hi + 1] - b0;
+        const bool local = nbins <= kPartBins;
+        if (local)
+            for (uint32_t j = threadIdx.x; j < nbins; j += kPartThreads) bins[j] = 0;
+        __syncthreads();
+        for (uint64_t i = c0 + threadIdx.x; i < c1; i += kPartThreads) {
+            uint32_t s = lo;
+            if (hi != lo) s = lo + upper_index(set_key + lo, hi - lo + 1, i);
+            const uint64_t nb = set_bucket[s + 1] - set_bucket[s];
+            const uint32_t b = (uint32_t)(set_bucket[s] + remap128(keys[i].x, nb));
+            bucket_id[i] = b;
+            if (local) atomicAdd(&bins[b - b0], 1u);
+            else atomicAdd(&counts[b], 1u);
+        }
+        __syncthreads();
+        if (local)
+            for (uint32_t j = threadIdx.x; j < nbins; j += kPartThreads)
+                if (bins[j]) atomicAdd(&counts[b0 + j], bins[j]);
     }
 }
 
@@ -284,16 +305,18 @@ void launch_set_nbuckets(const uint64_t *set_key, uint32_t nsets, uint64_t bucke
 void launch_set_bucket_ids(const uint64_t *keys128, uint64_t n, const uint64_t *set_key, const uint64_t *set_bucket,
                            uint32_t nsets, uint64_t nb_total, uint32_t *bucket_id, uint32_t *counts, cudaStream_t st) {
     cudaMemsetAsync(counts, 0, nb_total * sizeof(uint32_t), st);
-    k_set_bucket_ids<<<grid_for(n, 256, 148 * 16), 256, 0, st>>>((const ulonglong2 *)keys128, n, set_key, set_bucket,
-                                                                 nsets, bucket_id, counts);
+    k_set_bucket_ids<<<grid_for(n, kPartChunk, 148 * 6), kPartThreads, 0, st>>>((const ulonglong2 *)keys128, n, set_key,
+                                                                                set_bucket, nsets, bucket_id, counts);
     count_launches(1);
 }
 
-void launch_set_scatter(const uint64_t *keys128, uint64_t n, const uint32_t *bucket_id, const uint64_t *acc,
-                        uint32_t *cursor, uint64_t nb_total, uint64_t *sorted, cudaStream_t st) {
+void launch_set_scatter(const uint64_t *keys128, uint64_t n, const uint64_t *set_key, const uint64_t *set_bucket,
+                        uint32_t nsets, const uint32_t *bucket_id, const uint64_t *acc, uint32_t *cursor,
+                        uint64_t nb_total, uint64_t *sorted, cudaStream_t st) {
     cudaMemsetAsync(cursor, 0, nb_total * sizeof(uint32_t), st);
-    k_set_scatter<<<grid_for(n, 256, 148 * 16), 256, 0, st>>>((const ulonglong2 *)keys128, n, bucket_id, acc, cursor,
-                                                              sorted);
+    const SetBuckets map{set_key, set_bucket, nsets, bucket_id};
+    k_chunk_scatter<<<grid_for(n, kPartChunk, 148 * 6), kPartThreads, 0, st>>>((const ulonglong2 *)keys128, n, map, acc,
+                                                                               cursor, sorted);
     count_launches(1);
 }
 

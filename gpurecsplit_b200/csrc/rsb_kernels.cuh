@@ -33,7 +33,9 @@ void launch_bucket_count(const uint64_t *keys128, uint64_t n, uint64_t nbuckets,
 void launch_bucket_check(const uint32_t *counts, uint64_t nbuckets, DevStatus *status, cudaStream_t st);
 void launch_bucket_scatter(const uint64_t *keys128, uint64_t n, uint64_t nbuckets, const uint64_t *acc,
                            uint32_t *cursor, uint64_t *sorted, cudaStream_t st);
-void launch_bucket_sort(uint64_t *sorted, const uint64_t *acc, uint64_t nbuckets, DevStatus *status, cudaStream_t st);
+// Fails the build with RSB_ERR_DUPLICATE_KEY if a bucket holds two equal second halves.
+void launch_bucket_dupcheck(const uint64_t *sorted, const uint64_t *acc, uint64_t nbuckets, DevStatus *status,
+                            cudaStream_t st);
 void launch_bucket_nodes(const uint64_t *acc, uint64_t nbuckets, DevTables tab, uint32_t *node_count, cudaStream_t st);
 void launch_tree_emit(const uint64_t *acc, uint64_t nbuckets, const uint64_t *node_base, Shape sh, NodeArrays nodes,
                       cudaStream_t st);
@@ -96,8 +98,9 @@ void launch_evals(const uint64_t *node_total, NodeArrays nodes, uint32_t leaf, u
 void launch_set_nbuckets(const uint64_t *set_key, uint32_t nsets, uint64_t bucket_size, uint32_t *nb, cudaStream_t st);
 void launch_set_bucket_ids(const uint64_t *keys128, uint64_t n, const uint64_t *set_key, const uint64_t *set_bucket,
                            uint32_t nsets, uint64_t nb_total, uint32_t *bucket_id, uint32_t *counts, cudaStream_t st);
-void launch_set_scatter(const uint64_t *keys128, uint64_t n, const uint32_t *bucket_id, const uint64_t *acc,
-                        uint32_t *cursor, uint64_t nb_total, uint64_t *sorted, cudaStream_t st);
+void launch_set_scatter(const uint64_t *keys128, uint64_t n, const uint64_t *set_key, const uint64_t *set_bucket,
+                        uint32_t nsets, const uint32_t *bucket_id, const uint64_t *acc, uint32_t *cursor,
+                        uint64_t nb_total, uint64_t *sorted, cudaStream_t st);
 void launch_set_desc_words(const uint64_t *pos_acc, const uint64_t *set_bucket, uint32_t nsets, uint32_t *words,
                            uint64_t *set_bits, cudaStream_t st);
 void launch_set_write_rice(const uint64_t *node_base, uint64_t nb_total, NodeArrays nodes, DevTables tab,

@@ -6,6 +6,7 @@
 //   sort + partition          AbstractParallelRecSplit.hpp:339-359, src/Sorter.cpp:4-5
 //   grouping by bucket size   GPURecSplit.cuh:675-695
 #include "rsb_kernels.cuh"
+#include "rsb_partition.cuh"
 #include "rsb_spooky.cuh"
 
 namespace rsb {
@@ -172,52 +173,50 @@ __global__ void k_bucket_check(const uint32_t *counts, uint64_t nb, DevStatus *s
         if (counts[b] >= (uint32_t)kMaxBucketSize) set_error(status, RSB_ERR_BUCKET_TOO_LARGE, b);
 }
 
-__global__ void k_bucket_scatter(const ulonglong2 *__restrict__ keys, uint64_t n, uint64_t nb, const uint64_t *acc,
-                                 uint32_t *cursor, uint64_t *sorted) {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const ulonglong2 k = keys[i];
-        const uint64_t b = remap128(k.x, nb);
-        sorted[acc[b] + atomicAdd(&cursor[b], 1u)] = k.y;
-    }
-}
-
-// Sorts the `second` halves inside each bucket (bitonic network in shared memory) and
-// reports equal neighbours: two keys with the same second half in one bucket always
-// collide, so the reference's search would never end (GPURecSplit.cuh:436).
+// Duplicate check: two keys with the same second half in one bucket always collide, so the
+// reference's search would never end (GPURecSplit.cuh:436); here the build fails with
+// RSB_ERR_DUPLICATE_KEY. Each CTA inserts a bucket's second halves into an open-addressing
+// table in shared memory (read-only pass over the keys). The key order inside a bucket is
+// left as the scatter produced it: every seed depends only on the set of a node's keys.
 constexpr int kSortThreads = 256;
-constexpr int kSortCap = 4096;
+constexpr int kSortCap = 4096;  // > 2 * (kMaxBucketSize - 1) / 1.5: table at most 3/4 full
+constexpr uint64_t kEmptyKey = ~0ull;
+static_assert(4 * (kMaxBucketSize - 1) <= 3 * kSortCap, "duplicate table too small");
 
-__global__ void __launch_bounds__(kSortThreads) k_bucket_sort(uint64_t *sorted, const uint64_t *acc, uint64_t nb,
-                                                              DevStatus *status) {
-    __shared__ uint64_t s[kSortCap];
+__global__ void __launch_bounds__(kSortThreads) k_bucket_dupcheck(const uint64_t *sorted, const uint64_t *acc,
+                                                                  uint64_t nb, DevStatus *status) {
+    __shared__ uint64_t tab[kSortCap];
+    __shared__ uint32_t n_empty_key;  // keys equal to the empty-slot marker
     for (uint64_t b = blockIdx.x; b < nb; b += gridDim.x) {
         const uint64_t off = acc[b];
         const uint32_t m = (uint32_t)(acc[b + 1] - off);
-        if (m <= 1) continue;
-        if (m > (uint32_t)kSortCap) continue;  // rejected by k_bucket_check
-        uint32_t p = 1;
-        while (p < m) p <<= 1;
-        for (uint32_t i = threadIdx.x; i < p; i += kSortThreads) s[i] = i < m ? sorted[off + i] : ~0ull;
+        if (m <= 1 || m > (uint32_t)kMaxBucketSize) continue;  // oversize buckets: k_bucket_check
+        uint32_t size = 64;
+        while (size < 2 * m && size < (uint32_t)kSortCap) size <<= 1;
+        for (uint32_t i = threadIdx.x; i < size; i += kSortThreads) tab[i] = kEmptyKey;
+        if (threadIdx.x == 0) n_empty_key = 0;
         __syncthreads();
-        for (uint32_t k = 2; k <= p; k <<= 1) {
-            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-                for (uint32_t t = threadIdx.x; t < p / 2; t += kSortThreads) {
-                    const uint32_t i = 2 * t - (t & (j - 1));  // lower index of the pair
-                    const uint32_t l = i + j;
-                    const bool up = (i & k) == 0;
-                    const uint64_t a = s[i], c = s[l];
-                    if ((a > c) == up) {
-                        s[i] = c;
-                        s[l] = a;
-                    }
+        bool dup = false;
+        for (uint32_t i = threadIdx.x; i < m; i += kSortThreads) {
+            const uint64_t k = sorted[off + i];
+            if (k == kEmptyKey) {
+                dup |= atomicAdd(&n_empty_key, 1u) > 0;
+                continue;
+            }
+            // `second` is a hash output, so its low bits are a uniform slot; linear probing
+            // visits at most `size` slots and the table is at most 3/4 full.
+            uint32_t slot = (uint32_t)k & (size - 1);
+            for (uint32_t probe = 0; probe < size; ++probe) {
+                const uint64_t prev = atomicCAS((unsigned long long *)&tab[slot], kEmptyKey, k);
+                if (prev == kEmptyKey) break;
+                if (prev == k) {
+                    dup = true;
+                    break;
                 }
-                __syncthreads();
+                slot = (slot + 1) & (size - 1);
             }
         }
-        for (uint32_t i = threadIdx.x; i < m; i += kSortThreads) {
-            sorted[off + i] = s[i];
-            if (i + 1 < m && s[i] == s[i + 1]) set_error(status, RSB_ERR_DUPLICATE_KEY, b);
-        }
+        if (dup) set_error(status, RSB_ERR_DUPLICATE_KEY, b);
         __syncthreads();
     }
 }
@@ -374,12 +373,14 @@ void launch_bucket_check(const uint32_t *counts, uint64_t nb, DevStatus *status,
 void launch_bucket_scatter(const uint64_t *keys128, uint64_t n, uint64_t nb, const uint64_t *acc, uint32_t *cursor,
                            uint64_t *sorted, cudaStream_t st) {
     cudaMemsetAsync(cursor, 0, nb * sizeof(uint32_t), st);
-    k_bucket_scatter<<<grid_for(n, 256, 148 * 16), 256, 0, st>>>((const ulonglong2 *)keys128, n, nb, acc, cursor, sorted);
+    k_chunk_scatter<<<grid_for(n, kPartChunk, 148 * 6), kPartThreads, 0, st>>>((const ulonglong2 *)keys128, n,
+                                                                               PlainBuckets{nb}, acc, cursor, sorted);
     count_launches(1);
 }
 
-void launch_bucket_sort(uint64_t *sorted, const uint64_t *acc, uint64_t nb, DevStatus *status, cudaStream_t st) {
-    k_bucket_sort<<<grid_for(nb, 1, 148 * 6), kSortThreads, 0, st>>>(sorted, acc, nb, status);
+void launch_bucket_dupcheck(const uint64_t *sorted, const uint64_t *acc, uint64_t nb, DevStatus *status,
+                            cudaStream_t st) {
+    k_bucket_dupcheck<<<grid_for(nb, 1, 148 * 7), kSortThreads, 0, st>>>(sorted, acc, nb, status);
     count_launches(1);
 }
 
