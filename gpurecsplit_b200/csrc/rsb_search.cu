@@ -439,7 +439,7 @@ __global__ void __launch_bounds__(kThreads) k_partition_aggr(SearchCtx c) {
 // for the few collision-free ones; phase B computes their right masks and rotations.
 // Brute-force leaves: the first x whose m bit positions are all distinct.
 // ---------------------------------------------------------------------------------------
-constexpr int kLeafSeedsPerLane = 4;
+constexpr int kLeafSeedsPerLane = 8;
 constexpr int kLeafQueueCap = 32 + 32 * kLeafSeedsPerLane;
 
 template <int LEAF>
@@ -449,18 +449,22 @@ __device__ __forceinline__ uint32_t rotl_leaf(uint32_t v, uint32_t r) {
 }
 
 // Left masks of the S bases x0 + lane + 32 s of a rotation-leaf window (bu = SEED + x0*LEAF),
-// with the same per-key hoisting as moment_sums (the window spans 32*S*LEAF seeds).
+// with the same per-key hoisting as moment_sums (the window spans 32*S*LEAF seeds). The bit
+// of a key is remap16(key + seed, LEAF) = umulhi(hash16 << 16, LEAF), a multiply-high on
+// the FMA pipe beside the hash's ALU work.
 template <int LEAF, int S>
 __device__ __forceinline__ void left_masks(const uint64_t *sk, uint32_t nl, uint64_t bu, uint32_t *ml) {
     constexpr uint32_t kSpan = 32u * S * LEAF;
     static_assert(kSpan <= 0x10000u, "window wider than the hoisting allows");
     const uint32_t lane = threadIdx.x & 31;
+#pragma unroll 2
     for (uint32_t i = 0; i < nl; ++i) {
         const uint64_t tu = sk[i] + bu;
         const uint32_t lo0 = (uint32_t)tu, hi = (uint32_t)(tu >> 32);
         if ((lo0 & 0xFFFFu) > 0x10000u - kSpan) {
 #pragma unroll
-            for (int s = 0; s < S; ++s) ml[s] |= 1u << remap16(tu + (lane + 32u * s) * LEAF, LEAF);
+            for (int s = 0; s < S; ++s)
+                ml[s] |= 1u << __umulhi(hash16(tu + (lane + 32u * s) * LEAF) << 16, (uint32_t)LEAF);
         } else {
             const uint32_t K = hi ^ (hi >> 16) ^ (lo0 >> 16);
             const uint32_t l0 = lo0 + lane * LEAF;
@@ -470,7 +474,7 @@ __device__ __forceinline__ void left_masks(const uint64_t *sk, uint32_t nl, uint
                 z *= 0x85ebca6bu;
                 z ^= z >> 13;
                 z *= 0xc2b2ae35u;
-                ml[s] |= 1u << ((((z ^ (z >> 16)) & 0xFFFFu) * LEAF) >> 16);
+                ml[s] |= 1u << __umulhi((z << 16) ^ (z & 0xFFFF0000u), (uint32_t)LEAF);
             }
         }
     }
