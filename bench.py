@@ -13,11 +13,17 @@ keys (splitmix64, seed 42 + rank) with leaf size 16, bucket size 2000 and rotati
   roofline  the dominant search kernel's algorithmic evaluation rate (sum over its nodes
           of candidates x node size / its device time) against the device's measured
           remixAndRemap32 evaluation ceiling (rsb_probe_eval_rate)
-  cpu_baseline  the scalar CPU oracle (restatement of SIMDRecSplit, all host cores) on a
+  cpu_baseline  SIMDRecSplit restated on all host cores (the CPU oracle with its seed
+          searches in AVX-512 intrinsics; the scalar oracle on CPUs without AVX-512) on a
           bounded sample of the same workload
 
-`--impl reference` times only the CPU implementation of the path (the oracle port; the
-reference's own SIMDRecSplit cannot be compiled here: its submodules are absent).
+`--impl reference` times only that CPU implementation of the path (the reference's own
+SIMDRecSplit cannot be compiled here: its submodules are absent).
+
+Other modes (one JSON line each): `--mode batch` (many key sets in one pipeline vs
+back-to-back plain builds), `--mode serve` (continuous batching of string requests),
+`--mode c1` (1M printable string keys, l=8, b=100) and `--mode c3` (200k u64 keys, l=24,
+b=2000).
 
 Multi-GPU (torchrun): every rank builds its own 5M-key set (weak scaling, no data-path
 collective); the step time is the max over ranks.
@@ -343,6 +349,132 @@ def batch_workload(nsets: int, seed0: int = 1000):
     return keys, offsets
 
 
+# ---------------------------------------------------------------------------------------
+# Other plain configurations: C1 (string keys, l=8, b=100) and C3 (l=24)
+# ---------------------------------------------------------------------------------------
+def printable_strings(seed: int, n: int, min_len: int = 10, max_len: int = 50):
+    """n printable strings from one splitmix64 stream started at `seed`: per key one output
+    for the length (min_len + v % (max_len - min_len + 1)), then one output per byte
+    (0x21 + v % 94)."""
+    stream = splitmix64_keys(seed, n * (max_len + 1))
+    span = np.uint64(max_len - min_len + 1)
+    len_pos = np.empty(n, dtype=np.int64)
+    lens = np.empty(n, dtype=np.int64)
+    pos = 0
+    for i in range(n):  # each length decides where the next one is drawn
+        ln = min_len + int(stream[pos] % span)
+        len_pos[i] = pos
+        lens[i] = ln
+        pos += 1 + ln
+    is_byte = np.ones(pos, dtype=bool)
+    is_byte[len_pos] = False
+    data = (np.uint64(0x21) + stream[:pos][is_byte] % np.uint64(94)).astype(np.uint8)
+    offsets = np.zeros(n + 1, dtype=np.uint64)
+    offsets[1:] = np.cumsum(lens)
+    return data, offsets
+
+
+CONFIGS = {
+    # name: (key kind, seed, n, leaf, bucket, golden digest entry)
+    "c1": ("strings", 42, 1_000_000, 8, 100, "strings_n1M_l8_b100"),
+    "c3": ("u64", 43, 200_000, 24, 2000, "u64_n200k_l24_b2000"),
+}
+
+
+def run_config(args) -> None:
+    """Device build time of one plain configuration (keys resident in HBM, L2 flushed before
+    every timed step), end-to-end time from host keys, and parity with the oracle digest."""
+    import ctypes
+
+    import torch
+    import gpurecsplit_b200 as rsb
+
+    kind, seed, n, leaf, b, golden = CONFIGS[args.mode]
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    engine = rsb.Engine(0, stream.cuda_stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    L = rsb.lib()
+    if kind == "strings":
+        data, offsets = printable_strings(seed, n)
+        d_data = torch.from_numpy(data).to("cuda")
+        d_off = torch.from_numpy(offsets.view(np.int64)).to("cuda")
+        host_keys = (data, offsets)
+        flags = rsb.RSB_ROTATE | rsb.RSB_KEYS_ON_DEVICE | rsb.RSB_DEVICE_ONLY
+
+        def device_build():
+            h = ctypes.c_void_p()
+            rsb._check(L.rsb_build_strings(engine.handle, ctypes.c_void_p(d_data.data_ptr()),
+                                           ctypes.c_void_p(d_off.data_ptr()), n, b, leaf, flags, ctypes.byref(h)),
+                       "rsb_build_strings")
+            return rsb.GPURecSplit(bucket_size=b, leaf_size=leaf, _handle=h)
+        h2d = data.nbytes + offsets.nbytes
+    else:
+        keys = splitmix64_keys(seed, n)
+        d_keys = torch.from_numpy(keys.view(np.int64)).to("cuda")
+        host_keys = keys
+
+        def device_build():
+            return rsb.GPURecSplit.from_device(d_keys.data_ptr(), n, b, leaf, key_type="u64", engine=engine,
+                                               device_only=True)
+        h2d = keys.nbytes
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        flush.zero_()
+        device_build().close()
+    times, stats = [], None
+    with ClockSampler(0) as clocks:
+        for _ in range(args.steps):
+            flush.zero_()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            f = device_build()
+            e.record(stream)
+            e.synchronize()
+            times.append(s.elapsed_time(e))
+            stats = f.stats()
+            f.close()
+    e2e = []
+    blob = None
+    for i in range(3):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        f = rsb.GPURecSplit(host_keys, bucket_size=b, leaf_size=leaf, key_type=kind, engine=engine)
+        blob = f.serialize()
+        if i > 0:
+            e2e.append(time.perf_counter() - t0)
+        bits = f.get_bits()
+        f.close()
+    parity = None
+    if os.path.exists(GOLDEN):
+        g = json.load(open(GOLDEN)).get(golden)
+        if g is not None:
+            parity = {"sha256_equals_oracle": hashlib.sha256(blob).hexdigest() == g["sha256"], "golden": golden}
+    ms = statistics.median(times)
+    ms_search = stats["ms_search"]
+    line = {
+        "metric": f"build ns/key ({args.mode}: {kind} keys, l={leaf}, b={b}, n={n})", "value": ms * 1e6 / n,
+        "unit": "ns/key", "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": f"{kind} keys n={n} (splitmix64 seed {seed}"
+                               + (", printable 10-50 B strings" if kind == "strings" else "")
+                               + f"), l={leaf}, b={b}, rotation", "l2": "flushed before every timed step"},
+        "e2e": {"value": statistics.mean(e2e) * 1e9 / n, "unit": "ns/key", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": len(blob), "timing": "host wall clock around the public-API build"},
+        "bits_per_key": bits / n, "parity": parity,
+        "stage_ms": {"partition": stats["ms_partition"],
+                     "search": {str(i): round(v, 3) for i, v in enumerate(ms_search) if v > 0},
+                     "encode": stats["ms_encode"], "total": stats["ms_total"]},
+        "stage_geval_s": {str(i): round(stats["evals_stage"][i] / (v * 1e-3) / 1e9, 1)
+                          for i, v in enumerate(ms_search) if v > 0.05},
+        "gpu_launches": stats["kernel_launches"], "clocks": clocks.summary(),
+        "step_ms": [round(x, 3) for x in times],
+    }
+    print(json.dumps(line), flush=True)
+    engine.close()
+
+
 def run_batch(args) -> None:
     import torch
     import gpurecsplit_b200 as rsb
@@ -544,7 +676,7 @@ def main() -> None:
     ap.add_argument("--cpu-buckets", type=int, default=None, help="CPU baseline sample (default 192, 48 without AVX-512)")
     ap.add_argument("--ref-buckets", type=int, default=None, help="reference-arm sample (default 96, 24 without AVX-512)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="plain", choices=["plain", "batch", "serve"])
+    ap.add_argument("--mode", default="plain", choices=["plain", "batch", "serve", "c1", "c3"])
     ap.add_argument("--sets", type=int, default=1000)
     ap.add_argument("--requests", type=int, default=100)
     ap.add_argument("--max-keys", type=int, default=10_000_000)
@@ -557,6 +689,10 @@ def main() -> None:
         return
     if args.mode == "serve":
         run_serve(args)
+        return
+    if args.mode in CONFIGS:
+        args.warmup = max(args.warmup, 3)
+        run_config(args)
         return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
