@@ -68,6 +68,26 @@ def splitmix64_keys(seed: int, n: int) -> np.ndarray:
         return z ^ (z >> np.uint64(31))
 
 
+def rank_keys(rank: int, n: int) -> np.ndarray:
+    """The keys rank `rank` builds: replicas get independent sets (splitmix64 seed 42 + rank)."""
+    return splitmix64_keys(SEED + rank, n)
+
+
+def max_over_ranks(x: float, dist=None, device: str = "cpu") -> float:
+    """The maximum of x over all ranks (x itself without a process group)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def ns_per_key(total_ms: float, steps: int, n: int, world: int) -> float:
+    """Whole-job ns/key: the slowest rank's time per step over the keys of all ranks."""
+    return total_ms / steps * 1e6 / (n * world)
+
+
 def workload_config(n: int, world: int) -> dict:
     return {
         "workload": f"u64 keys n={n} (splitmix64 seed 42+rank) hashed to 128 bits (fmix64 / stafford13), "
@@ -198,7 +218,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
     stream = torch.cuda.current_stream()
     engine = rsb.Engine(local_rank, stream.cuda_stream)
     n = args.n
-    keys_host = splitmix64_keys(SEED + rank, n)
+    keys_host = rank_keys(rank, n)
     pinned = torch.from_numpy(keys_host.view(np.int64)).pin_memory()
     keys_dev = pinned.to(f"cuda:{local_rank}")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local_rank}")
@@ -237,13 +257,9 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
             last = f
         barrier()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms = sum(step_ms)
-    if dist is not None:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(step_ms), dist, f"cuda:{local_rank}")
     ms_per_step = total_ms / args.steps
-    value = ms_per_step * 1e6 / (n * world)
+    value = ns_per_key(total_ms, args.steps, n, world)
 
     # parity of the last timed build with the committed oracle digest
     parity = None
@@ -277,12 +293,8 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         # the status word, encoder parameters and stage counts read at the end of the build
         d2h_bytes = len(blob) - 8 * 14 + 16 + 8 * 36 + 4 * 21
         f.close()
-    e2e_total = sum(e2e_ms)
-    if dist is not None:
-        t = torch.tensor([e2e_total], dtype=torch.float64, device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e_value = e2e_total / e2e_steps * 1e6 / (n * world)
+    e2e_total = max_over_ranks(sum(e2e_ms), dist, f"cuda:{local_rank}")
+    e2e_value = ns_per_key(e2e_total, e2e_steps, n, world)
 
     if rank == 0:
         # ---- roofline of the dominant search kernel ----
