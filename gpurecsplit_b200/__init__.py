@@ -87,6 +87,7 @@ def lib():
             "rsb_engine_destroy": ([vp], i32),
             "rsb_engine_set_budget": ([vp, u32, u64], i32),
             "rsb_engine_reserve": ([vp, u64, u64, u64, u32], i32),
+            "rsb_engine_set_occupancy": ([vp, u32], i32),
             "rsb_build_hash128": ([vp, vp, u64, u64, u32, u32, pp], i32),
             "rsb_build_strings": ([vp, vp, vp, u64, u64, u32, u32, pp], i32),
             "rsb_build_u64": ([vp, vp, u64, u64, u32, u32, pp], i32),
@@ -158,6 +159,10 @@ class Engine:
     def reserve(self, keys: int, bucket_size: int, string_bytes: int = 0, sets: int = 1) -> None:
         """Pre-sizes the device scratch for builds of up to `keys` keys (rsb_engine_reserve)."""
         _check(lib().rsb_engine_reserve(self._h, keys, bucket_size, string_bytes, sets), "rsb_engine_reserve")
+
+    def set_occupancy(self, percent: int) -> None:
+        """Runs the persistent search kernels at `percent` of full occupancy (rsb_engine_set_occupancy)."""
+        _check(lib().rsb_engine_set_occupancy(self._h, percent), "rsb_engine_set_occupancy")
 
     def probe_eval_rate(self):
         """(evaluations per second, ms) of the synthetic remixAndRemap32 ceiling kernel."""

@@ -78,6 +78,7 @@ struct rsb_engine {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     int num_sms = 0;
+    int occupancy_pct = 100;
     uint32_t budget_shift = 10;
     uint64_t budget_min = 1ull << 16;
     std::map<uint32_t, std::pair<uint32_t *, uint32_t *>> tables;  // (leaf, rotate) -> device memo, nodes
@@ -362,6 +363,7 @@ rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint
     sc.budget_shift = e->budget_shift;
     sc.budget_min = e->budget_min;
     sc.num_sms = e->num_sms;
+    sc.occupancy_pct = e->occupancy_pct;
     RSB_CKH(enqueue_searches(e, sc, lt, st));
 
     // ---- encoding ----
@@ -375,6 +377,11 @@ rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint
     launch_evals(node_total, nodes, leaf, rotate ? 1 : 0, e->efp.p, st);
     RSB_CKH(cudaGetLastError());
     RSB_CKH(cudaEventRecord(e->ev[kNumEvents - 1], st));
+    // Wait for the build before the pageable copies below: a device-to-host copy into pageable
+    // memory holds the calling thread inside the driver until its stream reaches it, which
+    // would also hold back other threads' pageable copies (another engine's build) for the
+    // whole duration of this build.
+    RSB_CKH(cudaEventSynchronize(e->ev[kNumEvents - 1]));
 
     DevStatus dst{};
     uint32_t stage_counts[kNumStages];
@@ -540,6 +547,7 @@ rsb_status build_batch_device(rsb_engine *e, const uint64_t *keys128, const uint
     sc.budget_shift = e->budget_shift;
     sc.budget_min = e->budget_min;
     sc.num_sms = e->num_sms;
+    sc.occupancy_pct = e->occupancy_pct;
     RSB_CK(enqueue_searches(e, sc, lt, st));
     // ---- per-set encoding ----
     launch_bucket_bits(e->node_base.p, nb_total, nodes, tab, e->bits.p, e->fixed_bits.p, e->status.p, st);
@@ -559,6 +567,11 @@ rsb_status build_batch_device(rsb_engine *e, const uint64_t *keys128, const uint
     launch_evals(node_total, nodes, leaf, rotate ? 1 : 0, e->efp.p, st);
     RSB_CK(cudaGetLastError());
     RSB_CK(cudaEventRecord(e->ev[kNumEvents - 1], st));
+    // Wait for the build before the pageable copies below: a device-to-host copy into pageable
+    // memory holds the calling thread inside the driver until its stream reaches it, which
+    // would also hold back other threads' pageable copies (another engine's build) for the
+    // whole duration of this build.
+    RSB_CK(cudaEventSynchronize(e->ev[kNumEvents - 1]));
 
     DevStatus dst{};
     EfParams totals{};
@@ -766,6 +779,12 @@ rsb_status rsb_engine_reserve(rsb_engine *e, uint64_t keys, uint64_t bucket_size
     return s;
 }
 
+rsb_status rsb_engine_set_occupancy(rsb_engine *e, uint32_t percent) {
+    if (!e || percent == 0 || percent > 100) return RSB_ERR_BAD_ARG;
+    e->occupancy_pct = (int)percent;
+    return RSB_OK;
+}
+
 static rsb_status stage_keys128(rsb_engine *e, const rsb_hash128 *keys, uint64_t n, uint32_t flags, const uint64_t **dk) {
     if (flags & RSB_KEYS_ON_DEVICE) {
         *dk = (const uint64_t *)keys;
@@ -933,6 +952,7 @@ rsb_status rsb_hash_strings(rsb_engine *e, const uint8_t *bytes, const uint64_t 
     if (s != RSB_OK) return s;
     launch_hash_strings(db, doff, n, sbase, e->keys128.p, e->stream);
     RSB_CK(cudaGetLastError());
+    RSB_CK(cudaStreamSynchronize(e->stream));  // before a pageable copy (see the build paths)
     RSB_CK(cudaMemcpyAsync(out, e->keys128.p, n * 16, (flags & RSB_KEYS_ON_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                            e->stream));
     RSB_CK(cudaStreamSynchronize(e->stream));
@@ -954,7 +974,8 @@ rsb_status rsb_hash_u64(rsb_engine *e, const uint64_t *keys, uint64_t n, uint32_
     launch_hash_u64(dk, n, e->keys128.p, e->stream);
     RSB_CK(cudaGetLastError());
     if (n)
-        RSB_CK(cudaMemcpyAsync(out, e->keys128.p, n * 16, (flags & RSB_KEYS_ON_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+        RSB_CK(cudaStreamSynchronize(e->stream));  // before a pageable copy (see the build paths)
+    RSB_CK(cudaMemcpyAsync(out, e->keys128.p, n * 16, (flags & RSB_KEYS_ON_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                                e->stream));
     RSB_CK(cudaStreamSynchronize(e->stream));
     return RSB_OK;

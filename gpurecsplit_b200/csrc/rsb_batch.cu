@@ -298,6 +298,7 @@ __global__ void __launch_bounds__(kEfThreads) k_set_ef_fill(const uint64_t *acc,
 }  // namespace
 
 void launch_set_nbuckets(const uint64_t *set_key, uint32_t nsets, uint64_t bucket_size, uint32_t *nb, cudaStream_t st) {
+    use_max_smem(k_set_nbuckets);
     k_set_nbuckets<<<grid_for(nsets, 256, 1024), 256, 0, st>>>(set_key, nsets, bucket_size, nb);
     count_launches(1);
 }
@@ -305,6 +306,7 @@ void launch_set_nbuckets(const uint64_t *set_key, uint32_t nsets, uint64_t bucke
 void launch_set_bucket_ids(const uint64_t *keys128, uint64_t n, const uint64_t *set_key, const uint64_t *set_bucket,
                            uint32_t nsets, uint64_t nb_total, uint32_t *bucket_id, uint32_t *counts, cudaStream_t st) {
     cudaMemsetAsync(counts, 0, nb_total * sizeof(uint32_t), st);
+    use_max_smem(k_set_bucket_ids);
     k_set_bucket_ids<<<grid_for(n, kPartChunk, 148 * 6), kPartThreads, 0, st>>>((const ulonglong2 *)keys128, n, set_key,
                                                                                 set_bucket, nsets, bucket_id, counts);
     count_launches(1);
@@ -315,6 +317,7 @@ void launch_set_scatter(const uint64_t *keys128, uint64_t n, const uint64_t *set
                         uint64_t nb_total, uint64_t *sorted, cudaStream_t st) {
     cudaMemsetAsync(cursor, 0, nb_total * sizeof(uint32_t), st);
     const SetBuckets map{set_key, set_bucket, nsets, bucket_id};
+    use_max_smem(k_chunk_scatter<SetBuckets>);
     k_chunk_scatter<<<grid_for(n, kPartChunk, 148 * 6), kPartThreads, 0, st>>>((const ulonglong2 *)keys128, n, map, acc,
                                                                                cursor, sorted);
     count_launches(1);
@@ -322,6 +325,7 @@ void launch_set_scatter(const uint64_t *keys128, uint64_t n, const uint64_t *set
 
 void launch_set_desc_words(const uint64_t *pos_acc, const uint64_t *set_bucket, uint32_t nsets, uint32_t *words,
                            uint64_t *set_bits, cudaStream_t st) {
+    use_max_smem(k_set_desc_words);
     k_set_desc_words<<<grid_for(nsets, 256, 1024), 256, 0, st>>>(pos_acc, set_bucket, nsets, words, set_bits);
     count_launches(1);
 }
@@ -330,6 +334,7 @@ void launch_set_write_rice(const uint64_t *node_base, uint64_t nb_total, NodeArr
                            const uint64_t *pos_acc, const uint32_t *fixed_bits, const uint64_t *set_bucket,
                            uint32_t nsets, const uint64_t *word_base, const uint64_t *set_bits, uint64_t *desc,
                            uint64_t cap_words, DevStatus *status, cudaStream_t st) {
+    use_max_smem(k_set_write_rice);
     k_set_write_rice<<<grid_for(nb_total * 32, 256, 148 * 8), 256, 0, st>>>(node_base, nb_total, nodes, tab, pos_acc,
                                                                           fixed_bits, set_bucket, nsets, word_base,
                                                                           set_bits, desc, cap_words, status);
@@ -340,6 +345,7 @@ void launch_set_ef_params(const uint64_t *acc, const uint64_t *pos, const uint64
                           EfParams *ef, uint32_t *lower_w, uint32_t *cum_w, uint32_t *pos_w, uint32_t *jump_w,
                           cudaStream_t st) {
     if (nsets == 0) return;
+    use_max_smem(k_set_ef_params);
     k_set_ef_params<<<nsets, kEfThreads, 0, st>>>(acc, pos, set_bucket, nsets, ef, lower_w, cum_w, pos_w, jump_w);
     count_launches(1);
 }
@@ -349,6 +355,7 @@ void launch_set_ef_fill(const uint64_t *acc, const uint64_t *pos, const uint64_t
                         const uint64_t *jump_base, uint64_t *lower, uint64_t *upper_cum, uint64_t *upper_pos,
                         uint64_t *jump, cudaStream_t st) {
     if (nsets == 0) return;
+    use_max_smem(k_set_ef_fill);
     k_set_ef_fill<<<nsets, kEfThreads, 0, st>>>(acc, pos, set_bucket, nsets, ef, lower_base, cum_base, pos_base,
                                                 jump_base, lower, upper_cum, upper_pos, jump);
     count_launches(1);

@@ -245,6 +245,7 @@ int grid_for(uint64_t n, int threads, int cap) {
 
 void launch_bucket_bits(const uint64_t *node_base, uint64_t nb, NodeArrays nodes, DevTables tab, uint32_t *bits,
                         uint32_t *fixed_bits, DevStatus *status, cudaStream_t st) {
+    use_max_smem(k_bucket_bits);
     k_bucket_bits<<<grid_for(nb * 32, 256, 148 * 8), 256, 0, st>>>(node_base, nb, nodes, tab, bits, fixed_bits, status);
     count_launches(1);
 }
@@ -252,6 +253,7 @@ void launch_bucket_bits(const uint64_t *node_base, uint64_t nb, NodeArrays nodes
 void launch_write_rice(const uint64_t *node_base, uint64_t nb, NodeArrays nodes, DevTables tab, const uint64_t *pos_acc,
                        const uint32_t *fixed_bits, uint64_t *desc, uint64_t desc_cap_words, EfParams *ef,
                        DevStatus *status, cudaStream_t st) {
+    use_max_smem(k_write_rice);
     k_write_rice<<<grid_for(nb * 32, 256, 148 * 8), 256, 0, st>>>(node_base, nb, nodes, tab, pos_acc, fixed_bits, desc,
                                                                    desc_cap_words, ef, status);
     count_launches(1);
@@ -260,15 +262,20 @@ void launch_write_rice(const uint64_t *node_base, uint64_t nb, NodeArrays nodes,
 void launch_ef_build(const uint64_t *cum, const uint64_t *pos, uint64_t nb, uint64_t /*keys*/, EfParams *ef,
                      uint64_t *lower, uint64_t lower_cap, uint64_t *upper_cum, uint64_t cum_cap, uint64_t *upper_pos,
                      uint64_t pos_cap, uint64_t *jump, uint64_t jump_cap, DevStatus *status, cudaStream_t st) {
+    use_max_smem(k_ef_init);
     k_ef_init<<<1, 32, 0, st>>>(cum, pos, nb, ef);
+    use_max_smem(k_ef_reduce);
     k_ef_reduce<<<grid_for(nb, 256, 148 * 4), 256, 0, st>>>(cum, pos, nb, ef);
+    use_max_smem(k_ef_params);
     k_ef_params<<<1, 32, 0, st>>>(cum, pos, nb, ef, lower_cap, cum_cap, pos_cap, jump_cap, status);
+    use_max_smem(k_ef_fill);
     k_ef_fill<<<grid_for(nb + 1, 256, 148 * 8), 256, 0, st>>>(cum, pos, nb, ef, lower, upper_cum, upper_pos, jump, status);
     count_launches(4);
 }
 
 void launch_evals(const uint64_t *node_total, NodeArrays nodes, uint32_t leaf, uint32_t rotate, EfParams *ef,
                   cudaStream_t st) {
+    use_max_smem(k_evals);
     k_evals<<<148 * 4, 256, 0, st>>>(node_total, nodes, leaf, rotate, ef);
     count_launches(1);
 }

@@ -8,6 +8,18 @@
 
 namespace rsb {
 
+// Every kernel of the engine asks for the largest shared-memory carveout of the SM (once per
+// kernel and device). An SM keeps one L1/shared split while CTAs are resident, so kernels of
+// two engines can only share SMs (a build service runs a small request beside a large one)
+// if neither kernel has the SMs configured with less shared memory than the other needs.
+// The kernels keep their working sets in shared memory and registers; L1 matters little.
+void prefer_shared_memory(const void *func);
+template <typename K>
+inline void use_max_smem(K kernel) {
+    prefer_shared_memory((const void *)kernel);
+}
+
+
 // Device-side per-leaf constants (uploaded once per engine and leaf size).
 struct DevTables {
     const uint32_t *memo;   // kMaxBucketSize
@@ -60,6 +72,7 @@ struct SearchCtx {
     uint32_t budget_shift;
     uint64_t budget_min;
     int num_sms;
+    int occupancy_pct;           // persistent kernels keep this percentage of full occupancy
 };
 void search_higher(const SearchCtx &c, int depth, cudaStream_t st);
 void search_aggr(const SearchCtx &c, int stage, cudaStream_t st);

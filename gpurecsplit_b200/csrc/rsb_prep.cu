@@ -5,6 +5,10 @@
 //   string hashing            GPURecSplit.cuh:443-468, util/Hash128.h:32-36
 //   sort + partition          AbstractParallelRecSplit.hpp:339-359, src/Sorter.cpp:4-5
 //   grouping by bucket size   GPURecSplit.cuh:675-695
+#include <mutex>
+#include <set>
+#include <utility>
+
 #include "rsb_kernels.cuh"
 #include "rsb_partition.cuh"
 #include "rsb_spooky.cuh"
@@ -60,7 +64,9 @@ __global__ void k_scan_reduce(const uint32_t *in, size_t n, uint64_t *block_sums
 }
 
 __global__ void k_scan_blocks(uint64_t *block_sums, size_t nblocks) {
-    // single block: exclusive scan of the block sums in place
+    // single block of kScanThreads: exclusive scan of the block sums in place. Every kernel of
+    // the engine keeps its CTA within 16K registers, so that it always fits beside another
+    // engine's persistent kernels running at 75 % of the SM (a build service's small lane).
     __shared__ uint64_t carry;
     __shared__ uint64_t tot;
     if (threadIdx.x == 0) carry = 0;
@@ -68,7 +74,7 @@ __global__ void k_scan_blocks(uint64_t *block_sums, size_t nblocks) {
     for (size_t b0 = 0; b0 < nblocks; b0 += blockDim.x) {
         const size_t i = b0 + threadIdx.x;
         const uint64_t v = i < nblocks ? block_sums[i] : 0;
-        const uint64_t ex = block_excl_scan<1024>(v, &tot);
+        const uint64_t ex = block_excl_scan<kScanThreads>(v, &tot);
         if (i < nblocks) block_sums[i] = carry + ex;
         __syncthreads();
         if (threadIdx.x == 0) carry += tot;
@@ -104,8 +110,11 @@ size_t scan_blocks(size_t n) { return (n + kScanTile - 1) / kScanTile + 1; }
 
 void exclusive_scan_u32(const uint32_t *in, uint64_t *out, size_t n, ScanTmp tmp, cudaStream_t st) {
     const size_t blocks = n == 0 ? 1 : (n + kScanTile - 1) / kScanTile;
+    use_max_smem(k_scan_reduce);
     k_scan_reduce<<<blocks, kScanThreads, 0, st>>>(in, n, tmp.block_sums);
-    k_scan_blocks<<<1, 1024, 0, st>>>(tmp.block_sums, blocks);
+    use_max_smem(k_scan_blocks);
+    k_scan_blocks<<<1, kScanThreads, 0, st>>>(tmp.block_sums, blocks);
+    use_max_smem(k_scan_final);
     k_scan_final<<<blocks, kScanThreads, 0, st>>>(in, n, tmp.block_sums, out);
     count_launches(3);
 }
@@ -344,12 +353,14 @@ int grid_for(uint64_t n, int threads, int cap) {
 }  // namespace
 
 void launch_hash_u64(const uint64_t *keys, uint64_t n, uint64_t *out128, cudaStream_t st) {
+    use_max_smem(k_hash_u64);
     k_hash_u64<<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(keys, n, (ulonglong2 *)out128);
     count_launches(1);
 }
 
 void launch_hash_strings(const uint8_t *bytes, const uint64_t *offsets, uint64_t n, uint64_t base, uint64_t *out128,
                          cudaStream_t st) {
+    use_max_smem(k_hash_strings);
     k_hash_strings<<<grid_for(n, 128, 148 * 32), 128, 0, st>>>(bytes, offsets, n, base, (ulonglong2 *)out128);
     count_launches(1);
 }
@@ -357,15 +368,18 @@ void launch_hash_strings(const uint8_t *bytes, const uint64_t *offsets, uint64_t
 void launch_bucket_count(const uint64_t *keys128, uint64_t n, uint64_t nb, uint32_t *counts, cudaStream_t st) {
     cudaMemsetAsync(counts, 0, nb * sizeof(uint32_t), st);
     if (nb <= kSmemHistMax) {
+        use_max_smem(k_bucket_count_smem);
         k_bucket_count_smem<<<grid_for(n, 512, 148 * 4), 512, nb * sizeof(uint32_t), st>>>((const ulonglong2 *)keys128, n,
                                                                                             nb, counts);
     } else {
+        use_max_smem(k_bucket_count_global);
         k_bucket_count_global<<<grid_for(n, 256, 148 * 16), 256, 0, st>>>((const ulonglong2 *)keys128, n, nb, counts);
     }
     count_launches(1);
 }
 
 void launch_bucket_check(const uint32_t *counts, uint64_t nb, DevStatus *status, cudaStream_t st) {
+    use_max_smem(k_bucket_check);
     k_bucket_check<<<grid_for(nb, 256, 148 * 8), 256, 0, st>>>(counts, nb, status);
     count_launches(1);
 }
@@ -373,6 +387,7 @@ void launch_bucket_check(const uint32_t *counts, uint64_t nb, DevStatus *status,
 void launch_bucket_scatter(const uint64_t *keys128, uint64_t n, uint64_t nb, const uint64_t *acc, uint32_t *cursor,
                            uint64_t *sorted, cudaStream_t st) {
     cudaMemsetAsync(cursor, 0, nb * sizeof(uint32_t), st);
+    use_max_smem(k_chunk_scatter<PlainBuckets>);
     k_chunk_scatter<<<grid_for(n, kPartChunk, 148 * 6), kPartThreads, 0, st>>>((const ulonglong2 *)keys128, n,
                                                                                PlainBuckets{nb}, acc, cursor, sorted);
     count_launches(1);
@@ -380,17 +395,20 @@ void launch_bucket_scatter(const uint64_t *keys128, uint64_t n, uint64_t nb, con
 
 void launch_bucket_dupcheck(const uint64_t *sorted, const uint64_t *acc, uint64_t nb, DevStatus *status,
                             cudaStream_t st) {
+    use_max_smem(k_bucket_dupcheck);
     k_bucket_dupcheck<<<grid_for(nb, 1, 148 * 7), kSortThreads, 0, st>>>(sorted, acc, nb, status);
     count_launches(1);
 }
 
 void launch_bucket_nodes(const uint64_t *acc, uint64_t nb, DevTables tab, uint32_t *node_count, cudaStream_t st) {
+    use_max_smem(k_bucket_nodes);
     k_bucket_nodes<<<grid_for(nb, 256, 148 * 8), 256, 0, st>>>(acc, nb, tab, node_count);
     count_launches(1);
 }
 
 void launch_tree_emit(const uint64_t *acc, uint64_t nb, const uint64_t *node_base, Shape sh, NodeArrays nodes,
                       cudaStream_t st) {
+    use_max_smem(k_tree_emit);
     k_tree_emit<<<grid_for(nb, 64, 148 * 16), 64, 0, st>>>(acc, nb, node_base, sh, nodes);
     count_launches(1);
 }
@@ -399,10 +417,29 @@ void launch_stage_lists(const uint8_t *stage, const uint64_t *total_nodes, uint3
                         uint32_t *lists, cudaStream_t st) {
     cudaMemsetAsync(stage_info, 0, 3 * kNumStages * sizeof(uint32_t), st);
     const int g = grid_for(max_nodes, 256, 148 * 8);
+    use_max_smem(k_stage_hist);
     k_stage_hist<<<g, 256, 0, st>>>(stage, total_nodes, stage_info);
+    use_max_smem(k_stage_bases);
     k_stage_bases<<<1, 32, 0, st>>>(stage_info);
+    use_max_smem(k_stage_scatter);
     k_stage_scatter<<<g, 256, 0, st>>>(stage, total_nodes, stage_info, lists);
     count_launches(3);
+}
+
+
+void prefer_shared_memory(const void *func) {
+    static std::mutex mu;
+    static std::set<std::pair<const void *, int>> done;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!done.insert({func, dev}).second) return;
+    if (cudaFuncSetAttribute(func, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared) !=
+        cudaSuccess)
+        cudaGetLastError();  // a preference only: launches work without it
 }
 
 }  // namespace rsb

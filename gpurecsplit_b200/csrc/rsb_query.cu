@@ -17,6 +17,7 @@ void launch_query_view(const MphfView &f, const uint64_t *keys128, uint64_t n, u
     uint64_t g = (n + 255) / 256;
     if (g < 1) g = 1;
     if (g > 148 * 16) g = 148 * 16;
+    use_max_smem(k_query);
     k_query<<<(int)g, 256, 0, st>>>(f, (const ulonglong2 *)keys128, n, out);
 }
 

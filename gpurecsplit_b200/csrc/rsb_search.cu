@@ -16,6 +16,7 @@
 // is evaluated completely, and successes are merged with atomicMin — so at kernel end each
 // node holds the minimum successful seed, independent of scheduling. No warp ever waits on
 // another warp: the kernels contain no spin loops.
+#include <algorithm>
 #include <cstdio>
 
 #include "rsb_kernels.cuh"
@@ -626,10 +627,57 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
 
 // ---- host-side dispatch -------------------------------------------------------------
 
+// Per-SM resources of the current device (registers, shared memory incl. the per-CTA
+// reserve, threads, CTA slots).
+struct SmResources {
+    long regs, smem, smem_reserved, threads, blocks;
+};
+
+SmResources sm_resources() {
+    static SmResources r{};
+    static bool done = false;
+    if (!done) {
+        int dev = 0;
+        cudaDeviceProp p{};
+        if (cudaGetDevice(&dev) == cudaSuccess && cudaGetDeviceProperties(&p, dev) == cudaSuccess) {
+            r = SmResources{p.regsPerMultiprocessor, (long)p.sharedMemPerMultiprocessor, (long)p.reservedSharedMemPerBlock,
+                            p.maxThreadsPerMultiProcessor, p.maxBlocksPerMultiProcessor};
+            done = true;
+        } else {
+            cudaGetLastError();
+        }
+    }
+    return r;
+}
+
+// Resident CTAs of a persistent kernel: full occupancy on every SM, or - when the engine
+// shares the GPU with another stream's persistent kernels - as many CTAs per SM as fit in
+// `pct` percent of EVERY per-SM resource (registers at warp allocation granularity, shared
+// memory with its per-CTA reserve, threads, CTA slots). Lanes whose percentages add up to
+// at most 100 therefore always fit side by side, and neither lane's grid has CTAs waiting
+// for the other lane's kernel to finish (a persistent kernel ends only after all of its CTAs
+// have started). At least one CTA per SM.
 template <typename K>
-int persistent_grid(K kernel, size_t smem, int num_sms, int threads = kThreads) {
+int persistent_grid(K kernel, size_t smem, int num_sms, int threads = kThreads, int pct = 100) {
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+    if (pct > 0 && pct < 100) {
+        cudaFuncAttributes a{};
+        const SmResources R = sm_resources();
+        if (cudaFuncGetAttributes(&a, kernel) == cudaSuccess && R.regs > 0) {
+            const long warps = (threads + 31) / 32;
+            const long cta_regs = warps * (((long)a.numRegs * 32 + 255) / 256) * 256;
+            const long cta_smem = (long)a.sharedSizeBytes + (long)smem + R.smem_reserved;
+            long cap = pct * R.blocks / 100;
+            if (cta_regs > 0) cap = std::min(cap, pct * R.regs / 100 / cta_regs);
+            cap = std::min(cap, pct * R.smem / 100 / cta_smem);
+            cap = std::min(cap, pct * R.threads / 100 / (warps * 32));
+            per_sm = (int)std::min<long>(per_sm, cap);
+        } else {
+            cudaGetLastError();
+            per_sm = per_sm * pct / 100;
+        }
+    }
     if (per_sm < 1) per_sm = 1;
     return per_sm * num_sms;
 }
@@ -641,20 +689,22 @@ void run_aggr(const SearchCtx &c, int stage, cudaStream_t st) {
         const size_t smem = kWarpsPerCta * C::WARP_WORDS * sizeof(uint64_t);
         auto k = k_search_aggr<LEAF, kStageUpper>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        int g = persistent_grid(k, smem, c.num_sms);
+        int g = persistent_grid(k, smem, c.num_sms, kThreads, c.occupancy_pct);
         g = min(g, (int)(c.nslots / kWarpsPerCta));
         SearchCtx cc = c;
         cc.nslots = g * kWarpsPerCta;
+        use_max_smem(k);
         k<<<g, kThreads, smem, st>>>(cc);
     } else {
         using C = AggrCfg<LEAF, kStageLower>;
         const size_t smem = kWarpsPerCta * C::WARP_WORDS * sizeof(uint64_t);
         auto k = k_search_aggr<LEAF, kStageLower>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        int g = persistent_grid(k, smem, c.num_sms);
+        int g = persistent_grid(k, smem, c.num_sms, kThreads, c.occupancy_pct);
         g = min(g, (int)(c.nslots / kWarpsPerCta));
         SearchCtx cc = c;
         cc.nslots = g * kWarpsPerCta;
+        use_max_smem(k);
         k<<<g, kThreads, smem, st>>>(cc);
     }
 }
@@ -666,13 +716,15 @@ void run_partition(const SearchCtx &c, int stage, cudaStream_t st) {
         const size_t smem = kWarpsPerCta * C::MAXM * sizeof(uint64_t);
         auto k = k_partition_aggr<LEAF, kStageUpper>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k<<<persistent_grid(k, smem, c.num_sms), kThreads, smem, st>>>(c);
+        use_max_smem(k);
+        k<<<persistent_grid(k, smem, c.num_sms, kThreads, c.occupancy_pct), kThreads, smem, st>>>(c);
     } else {
         using C = AggrCfg<LEAF, kStageLower>;
         const size_t smem = kWarpsPerCta * C::MAXM * sizeof(uint64_t);
         auto k = k_partition_aggr<LEAF, kStageLower>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k<<<persistent_grid(k, smem, c.num_sms), kThreads, smem, st>>>(c);
+        use_max_smem(k);
+        k<<<persistent_grid(k, smem, c.num_sms, kThreads, c.occupancy_pct), kThreads, smem, st>>>(c);
     }
 }
 
@@ -681,13 +733,15 @@ void run_leaves(const SearchCtx &c, int stage, cudaStream_t st) {
     SearchCtx cc = c;
     if (stage == kStageLeafRot) {
         auto k = k_search_leaf<LEAF, true>;
-        int g = min(persistent_grid(k, 0, c.num_sms), (int)(c.nslots / kWarpsPerCta));
+        int g = min(persistent_grid(k, 0, c.num_sms, kThreads, c.occupancy_pct), (int)(c.nslots / kWarpsPerCta));
         cc.nslots = g * kWarpsPerCta;
+        use_max_smem(k);
         k<<<g, kThreads, 0, st>>>(cc);
     } else {
         auto k = k_search_leaf<LEAF, false>;
-        int g = min(persistent_grid(k, 0, c.num_sms), (int)(c.nslots / kWarpsPerCta));
+        int g = min(persistent_grid(k, 0, c.num_sms, kThreads, c.occupancy_pct), (int)(c.nslots / kWarpsPerCta));
         cc.nslots = g * kWarpsPerCta;
+        use_max_smem(k);
         k<<<g, kThreads, 0, st>>>(cc);
     }
 }
@@ -729,7 +783,8 @@ bool shape_matches_kernels(const Shape &s) { return s.lower == lower_of((int)s.l
 void search_higher(const SearchCtx &c, int depth, cudaStream_t st) {
     const size_t smem = kMaxBucketSize * sizeof(uint64_t);
     cudaFuncSetAttribute(k_search_higher, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_search_higher<<<persistent_grid(k_search_higher, smem, c.num_sms, kHigherThreads), kHigherThreads, smem, st>>>(c,
+    use_max_smem(k_search_higher);
+    k_search_higher<<<persistent_grid(k_search_higher, smem, c.num_sms, kHigherThreads, c.occupancy_pct), kHigherThreads, smem, st>>>(c,
                                                                                                            depth);
     count_launches(1);
 }
@@ -780,6 +835,7 @@ void probe_eval_rate(int num_sms, uint64_t *out_evals, cudaStream_t st) {
     const int g = persistent_grid(k_probe, 0, num_sms) * 4;
     unsigned long long *sink = nullptr;
     cudaMallocAsync((void **)&sink, 8, st);
+    use_max_smem(k_probe);
     k_probe<<<g, kThreads, 0, st>>>(sink);
     cudaFreeAsync(sink, st);
     count_launches(1);

@@ -12,6 +12,14 @@
 // bytes, buckets, sets) derived from its share, and a batch is admitted only while it fits
 // that capacity, so engines never grow and the server holds about hbm_budget bytes of
 // device memory from creation to destruction.
+//
+// Lanes: with two or more workers, worker 0 serves only small requests (estimated device
+// time below kSmallMs) on a high-priority stream, and the other workers take any request.
+// The persistent search kernels of the large lanes keep kLargeLaneOccupancy percent of full
+// occupancy and those of the small lane the rest, so a small request's grid is resident
+// beside a running large build instead of queueing CTAs behind it (a persistent kernel
+// cannot finish before all of its CTAs have started). A small request therefore never waits
+// for a multi-second batch to finish.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -23,11 +31,32 @@
 #include <unordered_map>
 #include <vector>
 
+#include <cmath>
+
+#include <cuda_runtime.h>
+
 #include "rsb.h"
 
 namespace {
 
 using Clock = std::chrono::steady_clock;
+
+constexpr double kSmallMs = 20.0;
+constexpr uint32_t kLargeLaneOccupancy = 75;
+
+// Device ns per key of a build by leaf size, interpolated geometrically between rates
+// measured on one B200 (l = 8: 2, 12: 5, 16: 250, 24: 1e5 ns/key); used only to route
+// requests between lanes.
+double est_ns_per_key(uint32_t leaf) {
+    static const double L[4] = {8, 12, 16, 24}, V[4] = {2, 5, 250, 1e5};
+    if (leaf <= 8) return V[0];
+    for (int i = 0; i < 3; ++i)
+        if (leaf <= L[i + 1]) {
+            const double t = (leaf - L[i]) / (L[i + 1] - L[i]);
+            return std::exp(std::log(V[i]) + t * (std::log(V[i + 1]) - std::log(V[i])));
+        }
+    return V[3];
+}
 
 struct Request {
     uint64_t id = 0;
@@ -39,6 +68,7 @@ struct Request {
     std::vector<uint64_t> offsets;   // n + 1 entries into bytes
     std::vector<rsb_hash128> keys;   // hash128 keys
     uint64_t buckets = 0;            // buckets of this request's function
+    double est_ms = 0;               // estimated device time of a build alone
     double submit_s = 0, admit_s = 0, done_s = 0;
     uint32_t batch_requests = 0;
     uint64_t batch_keys = 0;
@@ -77,7 +107,9 @@ struct rsb_server {
     Capacity cap;
     Clock::time_point t0;
     std::vector<rsb_engine *> engines;
+    std::vector<cudaStream_t> streams;  // streams the server created for its engines
     std::vector<std::thread> workers;
+    bool lanes = false;                 // worker 0 serves small requests only
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<Request *> pending;
@@ -141,6 +173,10 @@ void build(rsb_engine *e, std::vector<Request *> &batch) {
     }
 }
 
+bool may_take(const rsb_server *S, size_t w, const Request *r) {
+    return !(S->lanes && w == 0) || r->est_ms < kSmallMs;
+}
+
 void worker(rsb_server *S, size_t w) {
     rsb_engine *e = S->engines[w];
     for (;;) {
@@ -148,9 +184,18 @@ void worker(rsb_server *S, size_t w) {
         uint64_t keys = 0;
         {
             std::unique_lock<std::mutex> lock(S->mu);
-            S->cv_work.wait(lock, [&] { return S->stopping || !S->pending.empty(); });
-            if (S->pending.empty()) return;  // stopping and drained
-            const Request first = *S->pending.front();
+            Request *oldest = nullptr;
+            S->cv_work.wait(lock, [&] {
+                oldest = nullptr;
+                for (Request *r : S->pending)
+                    if (may_take(S, w, r)) {
+                        oldest = r;
+                        break;
+                    }
+                return S->stopping || oldest != nullptr;
+            });
+            if (!oldest) return;  // stopping, and nothing left this worker may take
+            const Request *first = oldest;  // stays valid: it moves from the queue into the batch
             const Capacity &cap = S->cap;
             uint64_t bytes = 0, buckets = 0;
             for (auto it = S->pending.begin(); it != S->pending.end();) {
@@ -158,7 +203,7 @@ void worker(rsb_server *S, size_t w) {
                 const bool fits = keys + r->n <= cap.keys && bytes + r->bytes.size() <= cap.bytes &&
                                   buckets + r->buckets <= cap.buckets && batch.size() < cap.sets &&
                                   keys + r->n <= S->max_batch_keys;
-                if (r->same_class(first) && (batch.empty() || fits)) {
+                if (r->same_class(*first) && may_take(S, w, r) && (batch.empty() || fits)) {
                     batch.push_back(r);
                     keys += r->n;
                     bytes += r->bytes.size();
@@ -211,7 +256,7 @@ rsb_status enqueue(rsb_server *S, Request *r, uint64_t *id) {
         S->requests[r->id] = r;
         *id = r->id;
     }
-    S->cv_work.notify_one();
+    S->cv_work.notify_all();  // lanes differ in what they may take
     return RSB_OK;
 }
 
@@ -232,17 +277,32 @@ rsb_status rsb_server_create(int device, uint64_t hbm_budget, uint32_t inflight,
     S->max_batch_keys = max_batch_keys ? max_batch_keys : (uint64_t)1 << 31;
     S->cap = capacity_for(S->share);
     S->t0 = Clock::now();
+    S->lanes = inflight >= 2;
+    auto fail = [&](rsb_status st) {
+        for (auto *x : S->engines) rsb_engine_destroy(x);
+        for (auto s : S->streams) cudaStreamDestroy(s);
+        delete S;
+        return st;
+    };
     for (uint32_t i = 0; i < inflight; ++i) {
-        rsb_engine *e = nullptr;
-        rsb_status st = rsb_engine_create(device, nullptr, &e);
-        if (st == RSB_OK) {
-            st = rsb_engine_reserve(e, S->cap.keys, 16, S->cap.bytes, S->cap.sets);
-            if (st != RSB_OK) rsb_engine_destroy(e);
+        cudaStream_t stream = nullptr;
+        if (S->lanes && i == 0) {  // the small-request lane runs on the highest stream priority
+            int least = 0, greatest = 0;
+            if (cudaSetDevice(device) != cudaSuccess || cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess ||
+                cudaStreamCreateWithPriority(&stream, cudaStreamNonBlocking, greatest) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(RSB_ERR_NO_DEVICE);
+            }
+            S->streams.push_back(stream);
         }
+        rsb_engine *e = nullptr;
+        rsb_status st = rsb_engine_create(device, stream, &e);
+        if (st == RSB_OK && S->lanes)
+            st = rsb_engine_set_occupancy(e, i == 0 ? 100 - kLargeLaneOccupancy : kLargeLaneOccupancy);
+        if (st == RSB_OK) st = rsb_engine_reserve(e, S->cap.keys, 16, S->cap.bytes, S->cap.sets);
         if (st != RSB_OK) {
-            for (auto *x : S->engines) rsb_engine_destroy(x);
-            delete S;
-            return st;
+            if (e) rsb_engine_destroy(e);
+            return fail(st);
         }
         S->engines.push_back(e);
     }
@@ -268,6 +328,7 @@ rsb_status rsb_server_submit_strings(rsb_server *S, const uint8_t *bytes, const 
     r->offsets.resize(n + 1);
     for (uint64_t i = 0; i <= n; ++i) r->offsets[i] = offsets[i] - b0;
     r->buckets = std::max<uint64_t>(1, (n + bucket - 1) / bucket);
+    r->est_ms = n * est_ns_per_key(leaf) * 1e-6;
     return enqueue(S, r, id);
 }
 
@@ -282,6 +343,7 @@ rsb_status rsb_server_submit_hash128(rsb_server *S, const rsb_hash128 *keys, uin
     r->n = n;
     r->keys.assign(keys, keys + n);
     r->buckets = std::max<uint64_t>(1, (n + bucket - 1) / bucket);
+    r->est_ms = n * est_ns_per_key(leaf) * 1e-6;
     return enqueue(S, r, id);
 }
 
@@ -317,6 +379,7 @@ rsb_status rsb_server_destroy(rsb_server *S) {
     S->cv_work.notify_all();
     for (auto &t : S->workers) t.join();
     for (auto *e : S->engines) rsb_engine_destroy(e);
+    for (auto s : S->streams) cudaStreamDestroy(s);
     for (auto &kv : S->requests) {
         if (kv.second->result) rsb_free(kv.second->result);
         delete kv.second;

@@ -87,6 +87,11 @@ rsb_status rsb_engine_set_budget(rsb_engine *engine, uint32_t shift, uint64_t mi
  * Returns RSB_ERR_OOM, leaving the engine usable, if the device cannot hold it. */
 rsb_status rsb_engine_reserve(rsb_engine *engine, uint64_t keys, uint64_t bucket_size, uint64_t string_bytes,
                               uint32_t sets);
+/* Limits the engine's persistent seed-search kernels to `percent` (1..100, default 100) of
+ * their full occupancy on every SM (no reference counterpart), leaving room on each SM for
+ * kernels of other streams - e.g. small requests of a build service running beside a large
+ * build. Results do not change; only scheduling does. */
+rsb_status rsb_engine_set_occupancy(rsb_engine *engine, uint32_t percent);
 
 /* ---- construction ------------------------------------------------------------------ */
 

@@ -91,3 +91,8 @@ def test_server_without_device_fails_cleanly(rsb):
     with pytest.raises(rsb.RSBError) as e:
         rsb.Server(hbm_budget=1 << 30, inflight=2)
     assert e.value.name in ("NO_DEVICE", "CUDA")
+
+
+def test_engine_occupancy_argument_checks(rsb):
+    L = rsb.lib()
+    assert L.rsb_engine_set_occupancy(None, 50) == 1

@@ -240,3 +240,14 @@ def test_string_keys_as_slice_of_larger_buffer(rsb, oracle_mod, engine):
     first = (rebased[0], rebased[1][:5001])
     assert funcs[0].serialize() == rsb.GPURecSplit(first, bucket_size=100, leaf_size=8, key_type="strings",
                                                    engine=engine).serialize()
+
+
+@pytest.mark.parametrize("pct", [25, 75])
+def test_reduced_occupancy_same_function(rsb, oracle_mod, pct):
+    """Persistent kernels with fewer resident CTAs find the same minimum seeds."""
+    eng = rsb.Engine(0)
+    eng.set_occupancy(pct)
+    keys = oracle_mod.keygen_hash128(pct, 60_000)
+    f = rsb.GPURecSplit(keys, bucket_size=2000, leaf_size=16, engine=eng)
+    assert f.serialize() == oracle_mod.build_mphf(keys, 16, 2000).bytes.tobytes()
+    eng.close()
