@@ -276,7 +276,7 @@ rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint
     RSB_ENSURE(e->nwin, max_nodes);
     RSB_ENSURE(e->lists, max_nodes);
     RSB_ENSURE(e->stage_info, 3 * kNumStages);
-    RSB_ENSURE(e->sched, kNumStages);
+    RSB_ENSURE(e->sched, 2 * kNumStages);
     RSB_ENSURE(e->slots, nslots);
     RSB_ENSURE(e->bits, nb);
     RSB_ENSURE(e->fixed_bits, nb);
@@ -329,7 +329,7 @@ rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint
     if (hash_keys) hash_keys();
     RSB_CKH(cudaMemsetAsync(e->status.p, 0, sizeof(DevStatus), st));
     RSB_CKH(cudaMemsetAsync(e->efp.p, 0, sizeof(EfParams), st));
-    RSB_CKH(cudaMemsetAsync(e->sched.p, 0, kNumStages * sizeof(uint32_t), st));
+    RSB_CKH(cudaMemsetAsync(e->sched.p, 0, 2 * kNumStages * sizeof(uint32_t), st));
 
     // ---- buckets ----
     launch_bucket_count(keys128, n, nb, e->counts.p, st);
@@ -447,7 +447,7 @@ rsb_status ensure_batch_buffers(rsb_engine *e, uint64_t n, uint64_t nb_total, ui
     RSB_ENSURE(e->nwin, max_nodes);
     RSB_ENSURE(e->lists, max_nodes);
     RSB_ENSURE(e->stage_info, 3 * kNumStages);
-    RSB_ENSURE(e->sched, kNumStages);
+    RSB_ENSURE(e->sched, 2 * kNumStages);
     RSB_ENSURE(e->slots, nslots);
     RSB_ENSURE(e->bits, nb_total);
     RSB_ENSURE(e->fixed_bits, nb_total);
@@ -511,7 +511,7 @@ rsb_status build_batch_device(rsb_engine *e, const uint64_t *keys128, const uint
     if (hash_keys) hash_keys();
     RSB_CK(cudaMemsetAsync(e->status.p, 0, sizeof(DevStatus), st));
     RSB_CK(cudaMemsetAsync(e->efp.p, 0, sizeof(EfParams), st));
-    RSB_CK(cudaMemsetAsync(e->sched.p, 0, kNumStages * sizeof(uint32_t), st));
+    RSB_CK(cudaMemsetAsync(e->sched.p, 0, 2 * kNumStages * sizeof(uint32_t), st));
     RSB_CK(cudaMemcpyAsync(e->set_key.p, h_off, (nsets + 1) * 8, cudaMemcpyHostToDevice, st));
     // ---- buckets of all sets ----
     launch_set_nbuckets(e->set_key.p, nsets, bucket_size, e->set_nb.p, st);

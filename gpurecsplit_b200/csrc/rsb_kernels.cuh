@@ -66,7 +66,7 @@ struct SearchCtx {
     uint64_t *keys;              // bucket-partitioned key seconds
     DevTables tab;
     DevStatus *status;
-    uint32_t *sched;             // per-stage scheduler words (fresh-node counter per stage)
+    uint32_t *sched;             // per stage: fresh-node counter [0, kNumStages), finished nodes [kNumStages, 2*kNumStages)
     uint32_t *slots;             // help slots
     uint32_t nslots;
     uint32_t budget_shift;

@@ -11,7 +11,8 @@
 // partitions the node in place. Aggregation nodes and leaves are searched by persistent
 // warps: a node hands out ascending windows of W candidate seeds from an atomic counter;
 // the warp that took the node from the stage list owns it, and warps that run out of fresh
-// nodes help unfinished ones (taking further windows of the same node). A window whose
+// nodes help unfinished ones that have already handed out kHelpAfterWindows windows (taking
+// further windows of the same node). A window whose
 // first seed is not below the node's current best is never evaluated, every other window
 // is evaluated completely, and successes are merged with atomicMin — so at kernel end each
 // node holds the minimum successful seed, independent of scheduling. No warp ever waits on
@@ -26,6 +27,10 @@ namespace rsb {
 namespace {
 
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+// An owner opens its node to helpers only once it has taken this many windows: most small
+// nodes (leaf sizes <= 12) find their seed in the first window, where a helper's window
+// would be wasted, while long searches gain helpers after a negligible delay.
+constexpr uint32_t kHelpAfterWindows = 2;
 constexpr int kWarpsPerCta = 8;
 constexpr int kThreads = kWarpsPerCta * 32;
 
@@ -105,17 +110,41 @@ __device__ __forceinline__ uint64_t budget_for(const SearchCtx &c, uint32_t m) {
     return b > c.budget_min ? b : c.budget_min;
 }
 
-// Scans the help slots (node ids of owners, from a pseudo-random start) for a node of the
-// current stage whose search has not found a seed yet.
+// Merges a candidate seed into a node's seed. The warp whose merge first moves the seed off
+// kSeedNotFound (a success or a failure) counts the node as finished in `found`, the stage's
+// finished-node counter, so that idle warps can stop looking for nodes to help once every
+// node of the stage has a seed.
+__device__ __forceinline__ void merge_seed(uint64_t *node_seed, uint64_t v, uint32_t *found) {
+    const unsigned long long old = atomicMin((unsigned long long *)node_seed, (unsigned long long)v);
+    if (old == kSeedNotFound) atomicAdd(found, 1u);
+}
+
+// Scans the help slots of the launched warps (node ids of owners, from a pseudo-random
+// start, four slots per lane per step) for a node of the current stage whose search has not
+// found a seed yet.
 __device__ uint32_t find_help(const SearchCtx &c, uint32_t start) {
-    const int lane = threadIdx.x & 31;
-    for (uint32_t k = 0; k < c.nslots; k += 32) {
-        uint32_t idx = start + k + lane;
-        while (idx >= c.nslots) idx -= c.nslots;
-        const uint32_t nd = (k + lane < c.nslots) ? vload32(&c.slots[idx]) : kEmpty;
-        const bool cand = nd != kEmpty && vload64(&c.nodes.seed[nd]) == kSeedNotFound;
-        const unsigned b = __ballot_sync(0xffffffffu, cand);
-        if (b) return __shfl_sync(0xffffffffu, nd, __ffs(b) - 1);
+    constexpr uint32_t U = 4;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t nw = min(c.nslots, gridDim.x * (uint32_t)kWarpsPerCta);
+    start %= nw;
+    for (uint32_t k = 0; k < nw; k += 32 * U) {
+        uint32_t nd[U];
+#pragma unroll
+        for (uint32_t j = 0; j < U; ++j) {
+            const uint32_t off = k + j * 32 + lane;
+            uint32_t idx = start + off;
+            if (idx >= nw) idx -= nw;
+            nd[j] = off < nw ? vload32(&c.slots[idx]) : kEmpty;
+        }
+        uint64_t sd[U];
+#pragma unroll
+        for (uint32_t j = 0; j < U; ++j) sd[j] = nd[j] != kEmpty ? vload64(&c.nodes.seed[nd[j]]) : 0;
+        uint32_t pick = kEmpty;
+#pragma unroll
+        for (uint32_t j = 0; j < U; ++j)
+            if (pick == kEmpty && nd[j] != kEmpty && sd[j] == kSeedNotFound) pick = nd[j];
+        const unsigned b = __ballot_sync(0xffffffffu, pick != kEmpty);
+        if (b) return __shfl_sync(0xffffffffu, pick, __ffs(b) - 1);
     }
     return kEmpty;
 }
@@ -281,7 +310,7 @@ __device__ __forceinline__ bool aggr_exact(const uint64_t *sk, uint32_t m, uint3
 template <int LEAF, int STAGE>
 __device__ __forceinline__ void aggr_drain(const uint64_t *sk, uint64_t *q, uint32_t &qn, uint32_t take, uint32_t m,
                                            uint32_t fan, bool full, uint64_t seed, uint32_t tlo, uint32_t thi,
-                                           uint64_t best, uint64_t *node_seed) {
+                                           uint64_t best, uint64_t *node_seed, uint32_t *found) {
     using C = AggrCfg<LEAF, STAGE>;
     const int lane = threadIdx.x & 31;
     const bool active = lane < (int)take;
@@ -290,7 +319,7 @@ __device__ __forceinline__ void aggr_drain(const uint64_t *sk, uint64_t *q, uint
     bool ok = false;
     if (active && x < best) ok = aggr_exact<LEAF, STAGE, C::WIDE>(sk, m, fan, full, seed + x, tlo, thi);
     const uint64_t v = warp_min_u64(ok ? x : ~0ull);
-    if (lane == 0 && v != ~0ull) atomicMin((unsigned long long *)node_seed, (unsigned long long)v);
+    if (lane == 0 && v != ~0ull) merge_seed(node_seed, v, found);
     qn -= take;
 }
 
@@ -307,10 +336,11 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
     const uint32_t gw = blockIdx.x * kWarpsPerCta + warp;
     const uint32_t count = c.stage_info[STAGE];
     const uint32_t base = c.stage_info[kNumStages + STAGE];
+    uint32_t *found = &c.sched[kNumStages + STAGE];  // nodes of this stage with a seed
     const uint64_t seed = start_seed(C::SEED_INDEX);
     uint32_t rng = gw * 2654435761u + 12345u;
     uint32_t node = kEmpty, m = 0, fan = 0, tlo = 0, thi = 0, t1 = 0, mult = 0, qn = 0;
-    bool owner = false, full = false;
+    bool owner = false, published = false, full = false;
     uint64_t budget = 0;
     for (;;) {
         if (node == kEmpty) {
@@ -321,11 +351,12 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
             if (f < count) {
                 node = c.lists[base + f];
                 owner = true;
-                if (lane == 0) c.slots[gw] = node;
+                published = false;
             } else {
                 owner = false;
+                if (vload32(found) >= count) break;  // every node of the stage has a seed
                 rng = rng * 1664525u + 1013904223u;
-                node = find_help(c, rng % c.nslots);
+                node = find_help(c, rng);
                 if (node == kEmpty) break;
             }
             const uint32_t start = c.nodes.start[node];
@@ -351,15 +382,19 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
         uint32_t w = 0;
         if (lane == 0) w = atomicAdd(&c.nodes.next_win[node], 1u);
         w = __shfl_sync(0xffffffffu, w, 0);
+        if (owner && !published && w >= kHelpAfterWindows) {  // a long search: open it to helpers
+            if (lane == 0) c.slots[gw] = node;
+            published = true;
+        }
         const uint64_t x0 = (uint64_t)w * W;
         uint64_t best = vload64(&c.nodes.seed[node]);
         if (x0 >= best || x0 >= budget) {
             while (qn > 0) {
                 best = vload64(&c.nodes.seed[node]);
-                aggr_drain<LEAF, STAGE>(sk, q, qn, min(qn, 32u), m, fan, full, seed, tlo, thi, best, &c.nodes.seed[node]);
+                aggr_drain<LEAF, STAGE>(sk, q, qn, min(qn, 32u), m, fan, full, seed, tlo, thi, best, &c.nodes.seed[node], found);
             }
-            if (x0 < best && lane == 0) atomicMin((unsigned long long *)&c.nodes.seed[node], (unsigned long long)kSeedFailed);
-            if (owner && lane == 0) c.slots[gw] = kEmpty;
+            if (x0 < best && lane == 0) merge_seed(&c.nodes.seed[node], kSeedFailed, found);
+            if (owner && published && lane == 0) c.slots[gw] = kEmpty;
             node = kEmpty;
             continue;
         }
@@ -379,7 +414,7 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
         __syncwarp();
         while (qn >= 32) {
             best = vload64(&c.nodes.seed[node]);
-            aggr_drain<LEAF, STAGE>(sk, q, qn, 32u, m, fan, full, seed, tlo, thi, best, &c.nodes.seed[node]);
+            aggr_drain<LEAF, STAGE>(sk, q, qn, 32u, m, fan, full, seed, tlo, thi, best, &c.nodes.seed[node], found);
         }
     }
 }
@@ -485,7 +520,7 @@ __device__ __forceinline__ void left_masks(const uint64_t *sk, uint32_t nl, uint
 template <int LEAF>
 __device__ __forceinline__ void leaf_drain(const uint64_t *sk, uint32_t nl, const uint64_t *qb, const uint32_t *qm,
                                            uint32_t &qn, uint32_t take, uint64_t seed, uint64_t best,
-                                           uint64_t *node_seed) {
+                                           uint64_t *node_seed, uint32_t *found) {
     constexpr uint32_t full = (1u << LEAF) - 1;
     const int lane = threadIdx.x & 31;
     const bool active = lane < (int)take;
@@ -508,7 +543,7 @@ __device__ __forceinline__ void leaf_drain(const uint64_t *sk, uint32_t nl, cons
         }
     }
     enc = warp_min_u64(enc);
-    if (lane == 0 && enc != ~0ull) atomicMin((unsigned long long *)node_seed, (unsigned long long)enc);
+    if (lane == 0 && enc != ~0ull) merge_seed(node_seed, enc, found);
     qn -= take;
 }
 
@@ -528,10 +563,11 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
     const uint32_t gw = blockIdx.x * kWarpsPerCta + warp;
     const uint32_t count = c.stage_info[STAGE];
     const uint32_t base = c.stage_info[kNumStages + STAGE];
+    uint32_t *found = &c.sched[kNumStages + STAGE];  // nodes of this stage with a seed
     const uint64_t seed = start_seed(kNumStartSeeds - 1);
     uint32_t rng = gw * 2654435761u + 777u;
     uint32_t node = kEmpty, m = 0, nl = 0;
-    bool owner = false;
+    bool owner = false, published = false;
     uint64_t budget = 0;
     for (;;) {
         if (node == kEmpty) {
@@ -542,11 +578,12 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
             if (f < count) {
                 node = c.lists[base + f];
                 owner = true;
-                if (lane == 0) c.slots[gw] = node;
+                published = false;
             } else {
                 owner = false;
+                if (vload32(found) >= count) break;  // every node of the stage has a seed
                 rng = rng * 1664525u + 1013904223u;
-                node = find_help(c, rng % c.nslots);
+                node = find_help(c, rng);
                 if (node == kEmpty) break;
             }
             const uint32_t start = c.nodes.start[node];
@@ -569,6 +606,10 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
         uint32_t w = 0;
         if (lane == 0) w = atomicAdd(&c.nodes.next_win[node], 1u);
         w = __shfl_sync(0xffffffffu, w, 0);
+        if (owner && !published && w >= kHelpAfterWindows) {  // a long search: open it to helpers
+            if (lane == 0) c.slots[gw] = node;
+            published = true;
+        }
         const uint64_t x0 = (uint64_t)w * W;                   // first base (ROT) or seed of the window
         const uint64_t enc0 = ROT ? x0 * LEAF : x0;            // first encoded seed of the window
         uint64_t best = vload64(&c.nodes.seed[node]);
@@ -576,11 +617,11 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
             if (ROT) {
                 while (qn > 0) {
                     best = vload64(&c.nodes.seed[node]);
-                    leaf_drain<LEAF>(sk, nl, qb, qm, qn, min(qn, 32u), seed, best, &c.nodes.seed[node]);
+                    leaf_drain<LEAF>(sk, nl, qb, qm, qn, min(qn, 32u), seed, best, &c.nodes.seed[node], found);
                 }
             }
-            if (enc0 < best && lane == 0) atomicMin((unsigned long long *)&c.nodes.seed[node], (unsigned long long)kSeedFailed);
-            if (owner && lane == 0) c.slots[gw] = kEmpty;
+            if (enc0 < best && lane == 0) merge_seed(&c.nodes.seed[node], kSeedFailed, found);
+            if (owner && published && lane == 0) c.slots[gw] = kEmpty;
             node = kEmpty;
             continue;
         }
@@ -606,7 +647,7 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
             __syncwarp();
             while (qn >= 32) {
                 best = vload64(&c.nodes.seed[node]);
-                leaf_drain<LEAF>(sk, nl, qb, qm, qn, 32u, seed, best, &c.nodes.seed[node]);
+                leaf_drain<LEAF>(sk, nl, qb, qm, qn, 32u, seed, best, &c.nodes.seed[node], found);
             }
             continue;
         } else {
@@ -621,7 +662,7 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
         }
         off = __reduce_min_sync(0xffffffffu, off);
         if (off != 0xFFFFFFFFu && lane == 0)
-            atomicMin((unsigned long long *)&c.nodes.seed[node], (unsigned long long)(enc0 + off));
+            merge_seed(&c.nodes.seed[node], enc0 + off, found);
     }
 }
 
