@@ -101,6 +101,8 @@ def _configure(L):
     L.orc_keygen_strings.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
                                      ctypes.c_void_p, ctypes.c_void_p]
     L.orc_hash_strings.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]
+    L.orc_search_aggr.restype = ctypes.c_uint64
+    L.orc_search_aggr.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64]
     L.orc_remap16.restype = ctypes.c_uint32
     L.orc_remap16.argtypes = [ctypes.c_uint64, ctypes.c_uint32]
     return L
@@ -224,6 +226,14 @@ def hash_strings(data: np.ndarray, offsets: np.ndarray) -> np.ndarray:
     out = np.zeros((n, 2), dtype=np.uint64)
     lib().orc_hash_strings(_ptr(data), _ptr(offsets), n, _ptr(out))
     return out
+
+
+def search_aggr(seconds: np.ndarray, split: int, seed: int, simd: bool = False) -> int:
+    """Minimum seed (from `seed`) splitting the keys into parts of `split` keys (the last part
+    the rest), by the scalar or the AVX-512 search loop."""
+    k = np.ascontiguousarray(seconds, dtype=np.uint64)
+    L = simd_lib() if simd else lib()
+    return int(L.orc_search_aggr(_ptr(k), k.size, split, seed))
 
 
 def remap16(x: int, n: int) -> int:

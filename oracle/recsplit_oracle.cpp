@@ -1106,4 +1106,10 @@ void orc_hash_strings(const uint8_t *bytes, const uint64_t *offsets, uint64_t n,
 
 uint32_t orc_remap16(uint64_t x, uint32_t n) { return remap16(x, n); }
 
+// One aggregation-level search (the build's search_aggr) on m keys with parts of `split`
+// keys from `seed`: lets tests compare the scalar and AVX-512 builds on single nodes.
+uint64_t orc_search_aggr(const uint64_t *keys, uint32_t m, uint32_t split, uint64_t seed) {
+    return search::search_aggr(keys, m, split, seed);
+}
+
 }  // extern "C"

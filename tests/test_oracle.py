@@ -125,3 +125,20 @@ def test_simd_oracle_equals_scalar(oracle_mod, leaf, b, n, rot):
     s = oracle_mod.build_mphf(keys, leaf, b, rot, threads=4, simd=True)
     assert a.bytes.tobytes() == s.bytes.tobytes()
     assert np.array_equal(a.seeds, s.seeds)
+
+
+# Minimum seed of each node from `seed` below, found once by the scalar search (minutes).
+_FANOUT9_SEEDS = {(22, 190): 111351572, (23, 200): 33009561, (24, 200): 176426661}
+
+
+@pytest.mark.parametrize("leaf,m", sorted(_FANOUT9_SEEDS))
+def test_simd_oracle_fanout9_remainder(oracle_mod, leaf, m):
+    """A lower-aggregation node of fanout 9 whose last part is short: the ninth part is
+    implied by the packed counts of the other eight. Both searches start 40 candidates before
+    the node's minimum seed, so both must return exactly 40."""
+    if not oracle_mod.simd_supported():
+        pytest.skip("CPU lacks AVX-512 F/DQ/BW/VL/VPOPCNTDQ")
+    seconds = oracle_mod.keygen_hash128(leaf * 7 + m, m)[:, 1]
+    seed = (0x9E3779B97F4A7C15 * (leaf + 1) + _FANOUT9_SEEDS[(leaf, m)] - 40) & (2**64 - 1)
+    assert oracle_mod.search_aggr(seconds, leaf, seed) == 40
+    assert oracle_mod.search_aggr(seconds, leaf, seed, simd=True) == 40
