@@ -11,8 +11,7 @@
 // partitions the node in place. Aggregation nodes and leaves are searched by persistent
 // warps: a node hands out ascending windows of W candidate seeds from an atomic counter;
 // the warp that took the node from the stage list owns it, and warps that run out of fresh
-// nodes help unfinished ones that have already handed out kHelpAfterWindows windows (taking
-// further windows of the same node). A window whose
+// nodes help unfinished ones (taking further windows of the same node). A window whose
 // first seed is not below the node's current best is never evaluated, every other window
 // is evaluated completely, and successes are merged with atomicMin — so at kernel end each
 // node holds the minimum successful seed, independent of scheduling. No warp ever waits on
@@ -27,10 +26,6 @@ namespace rsb {
 namespace {
 
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;
-// An owner opens its node to helpers only once it has taken this many windows: most small
-// nodes (leaf sizes <= 12) find their seed in the first window, where a helper's window
-// would be wasted, while long searches gain helpers after a negligible delay.
-constexpr uint32_t kHelpAfterWindows = 2;
 constexpr int kWarpsPerCta = 8;
 constexpr int kThreads = kWarpsPerCta * 32;
 
@@ -340,7 +335,7 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
     const uint64_t seed = start_seed(C::SEED_INDEX);
     uint32_t rng = gw * 2654435761u + 12345u;
     uint32_t node = kEmpty, m = 0, fan = 0, tlo = 0, thi = 0, t1 = 0, mult = 0, qn = 0;
-    bool owner = false, published = false, full = false;
+    bool owner = false, full = false;
     uint64_t budget = 0;
     for (;;) {
         if (node == kEmpty) {
@@ -351,7 +346,7 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
             if (f < count) {
                 node = c.lists[base + f];
                 owner = true;
-                published = false;
+                if (lane == 0) c.slots[gw] = node;
             } else {
                 owner = false;
                 if (vload32(found) >= count) break;  // every node of the stage has a seed
@@ -382,10 +377,6 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
         uint32_t w = 0;
         if (lane == 0) w = atomicAdd(&c.nodes.next_win[node], 1u);
         w = __shfl_sync(0xffffffffu, w, 0);
-        if (owner && !published && w >= kHelpAfterWindows) {  // a long search: open it to helpers
-            if (lane == 0) c.slots[gw] = node;
-            published = true;
-        }
         const uint64_t x0 = (uint64_t)w * W;
         uint64_t best = vload64(&c.nodes.seed[node]);
         if (x0 >= best || x0 >= budget) {
@@ -394,7 +385,7 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
                 aggr_drain<LEAF, STAGE>(sk, q, qn, min(qn, 32u), m, fan, full, seed, tlo, thi, best, &c.nodes.seed[node], found);
             }
             if (x0 < best && lane == 0) merge_seed(&c.nodes.seed[node], kSeedFailed, found);
-            if (owner && published && lane == 0) c.slots[gw] = kEmpty;
+            if (owner && lane == 0) c.slots[gw] = kEmpty;
             node = kEmpty;
             continue;
         }
@@ -567,7 +558,7 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
     const uint64_t seed = start_seed(kNumStartSeeds - 1);
     uint32_t rng = gw * 2654435761u + 777u;
     uint32_t node = kEmpty, m = 0, nl = 0;
-    bool owner = false, published = false;
+    bool owner = false;
     uint64_t budget = 0;
     for (;;) {
         if (node == kEmpty) {
@@ -578,7 +569,7 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
             if (f < count) {
                 node = c.lists[base + f];
                 owner = true;
-                published = false;
+                if (lane == 0) c.slots[gw] = node;
             } else {
                 owner = false;
                 if (vload32(found) >= count) break;  // every node of the stage has a seed
@@ -606,10 +597,6 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
         uint32_t w = 0;
         if (lane == 0) w = atomicAdd(&c.nodes.next_win[node], 1u);
         w = __shfl_sync(0xffffffffu, w, 0);
-        if (owner && !published && w >= kHelpAfterWindows) {  // a long search: open it to helpers
-            if (lane == 0) c.slots[gw] = node;
-            published = true;
-        }
         const uint64_t x0 = (uint64_t)w * W;                   // first base (ROT) or seed of the window
         const uint64_t enc0 = ROT ? x0 * LEAF : x0;            // first encoded seed of the window
         uint64_t best = vload64(&c.nodes.seed[node]);
@@ -621,7 +608,7 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
                 }
             }
             if (enc0 < best && lane == 0) merge_seed(&c.nodes.seed[node], kSeedFailed, found);
-            if (owner && published && lane == 0) c.slots[gw] = kEmpty;
+            if (owner && lane == 0) c.slots[gw] = kEmpty;
             node = kEmpty;
             continue;
         }
