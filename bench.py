@@ -541,6 +541,8 @@ def run_batch(args) -> None:
         "stage_ms": {"partition": st["ms_partition"], "search": {str(i): round(v, 3) for i, v in
                                                                  enumerate(st["ms_search"]) if v > 0},
                      "encode": st["ms_encode"], "total": st["ms_total"]},
+        "stage_geval_s": {str(i): round(st["evals_stage"][i] / (v * 1e-3) / 1e9, 1)
+                          for i, v in enumerate(st["ms_search"]) if v > 0.05},
         "gpu_launches": st["kernel_launches"], "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)
