@@ -248,6 +248,7 @@ __global__ void __launch_bounds__(kHigherThreads) k_search_higher(SearchCtx c, i
 // final best is still fully checked and the minimum is unchanged.
 // ---------------------------------------------------------------------------------------
 constexpr int kAggrSeedsPerLane = 8;
+constexpr uint32_t kAbortChunk = 64;  // keys between checks of the node's best seed
 constexpr uint32_t kAggrWindow = 32 * kAggrSeedsPerLane;
 constexpr int kQueueCap = 32 + (int)kAggrWindow;  // < 32 pending after a drain + one window
 
@@ -393,8 +394,24 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
         uint32_t cnt[S];
 #pragma unroll
         for (int s = 0; s < S; ++s) cnt[s] = 0;
-        if (full) moment_sums<S, true>(sk, m, seed + x0, fan, cnt);
-        else moment_sums<S, false>(sk, m, seed + x0, mult, cnt);
+        // The keys go in chunks; after each chunk the window is abandoned if the node's best
+        // seed has dropped to x0 or below (another warp succeeded below this window), since
+        // then none of its candidates can lower the minimum.
+        bool abandoned = false;
+        for (uint32_t i0 = 0; i0 < m; i0 += kAbortChunk) {
+            const uint32_t len = min(kAbortChunk, m - i0);
+            if (full) moment_sums<S, true>(sk + i0, len, seed + x0, fan, cnt);
+            else moment_sums<S, false>(sk + i0, len, seed + x0, mult, cnt);
+            if (i0 + len < m) {
+                uint64_t b = 0;
+                if (lane == 0) b = vload64(&c.nodes.seed[node]);
+                if (__shfl_sync(0xffffffffu, b, 0) <= x0) {
+                    abandoned = true;
+                    break;
+                }
+            }
+        }
+        if (abandoned) continue;
 #pragma unroll
         for (int s = 0; s < S; ++s) {
             const bool pass = cnt[s] == t1;
