@@ -22,6 +22,7 @@
 // for a multi-second batch to finish.
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -30,8 +31,6 @@
 #include <thread>
 #include <unordered_map>
 #include <vector>
-
-#include <cmath>
 
 #include <cuda_runtime.h>
 
