@@ -242,24 +242,30 @@ __global__ void __launch_bounds__(kHigherThreads) k_search_higher(SearchCtx c, i
 // the part index equals sum_j j * size_j — a necessary condition that costs one or two
 // multiply-highs and an add per key (moment_sums) instead of a packed part count, and that
 // about 1 / (2.5 * sqrt(m * var(p))) of the seeds pass (1.9 % at m = 112, fanout 7).
-// Phase A applies it to every seed of a window (8 per lane); the survivors go to a per-warp
+// Phase A applies it to every seed of a window (8 or 12 per lane); the survivors go to a per-warp
 // queue in shared memory, and phase B gives each lane one queued seed for the exact part
 // count. A warp drains its queue before it leaves a node, so every seed below the node's
 // final best is still fully checked and the minimum is unchanged.
 // ---------------------------------------------------------------------------------------
-constexpr int kAggrSeedsPerLane = 8;
 constexpr uint32_t kAbortChunk = 64;  // keys between checks of the node's best seed
-constexpr uint32_t kAggrWindow = 32 * kAggrSeedsPerLane;
-constexpr int kQueueCap = 32 + (int)kAggrWindow;  // < 32 pending after a drain + one window
+
+// Candidates per lane of a window, by leaf size (measured on one B200): 12 amortise the
+// per-key work better where nodes need thousands of candidates or more (l = 16: 253 -> 247
+// ns/key; l = 12 batched: +1.5 % keys/s); at l <= 11 a node needs only a few hundred, so the
+// larger window's overshoot costs more (l = 8: 1.84 -> 1.93 ms per 1M keys) and 8 stay.
+__host__ __device__ constexpr int aggr_seeds_per_lane(int leaf) { return leaf >= 12 ? 12 : 8; }
 
 template <int LEAF, int STAGE>
 struct AggrCfg {
+    static constexpr int S = aggr_seeds_per_lane(LEAF);
+    static constexpr uint32_t W = 32u * S;                  // candidates of one window
+    static constexpr int QCAP = 32 + (int)W;                // < 32 pending after a drain + one window
     static constexpr uint32_t SPLIT = STAGE == kStageUpper ? lower_of(LEAF) : (uint32_t)LEAF;
     static constexpr uint32_t MAXM = STAGE == kStageUpper ? upper_of(LEAF) : lower_of(LEAF);
     static constexpr uint32_t MAXF = (MAXM + SPLIT - 1) / SPLIT;
     static constexpr bool WIDE = MAXF > 4;
     static constexpr uint64_t SEED_INDEX = STAGE == kStageUpper ? 17 : 18;
-    static constexpr uint32_t WARP_WORDS = MAXM + kQueueCap;  // keys + candidate queue
+    static constexpr uint32_t WARP_WORDS = MAXM + QCAP;  // keys + candidate queue
 };
 
 __device__ __forceinline__ uint64_t warp_min_u64(uint64_t v) {
@@ -322,8 +328,8 @@ __device__ __forceinline__ void aggr_drain(const uint64_t *sk, uint64_t *q, uint
 template <int LEAF, int STAGE>
 __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
     using C = AggrCfg<LEAF, STAGE>;
-    constexpr int S = kAggrSeedsPerLane;
-    constexpr uint32_t W = kAggrWindow;
+    constexpr int S = C::S;
+    constexpr uint32_t W = C::W;
     extern __shared__ uint64_t smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint64_t *sk = smem + warp * C::WARP_WORDS;
@@ -850,13 +856,13 @@ void search_leaves(const SearchCtx &c, int stage, cudaStream_t st) {
 // ---- eval-rate probe ------------------------------------------------------------------
 // The cheapest complete candidate evaluation of any search (key + seed, remix32, 16-bit
 // remap to a part index, sum) in the exact form of the aggregation filter (moment_sums on a
-// full node: keys broadcast from shared memory, 8 candidates per lane, unrolled key loop),
+// full node: keys broadcast from shared memory, 12 candidates per lane, unrolled key loop),
 // run at full occupancy with no scheduling, no queues and no reductions: the integer
 // ceiling for remixAndRemap32 evaluations on this device.
 namespace {
 constexpr int kProbeKeys = 128;
 constexpr int kProbeIters = 32;
-constexpr int kProbeSeeds = 8;
+constexpr int kProbeSeeds = 12;
 __global__ void __launch_bounds__(kThreads) k_probe(unsigned long long *sink) {
     __shared__ uint64_t sk[kProbeKeys];
     for (int i = threadIdx.x; i < kProbeKeys; i += kThreads) sk[i] = start_seed(i % 20) * (2 * i + 1);
