@@ -54,24 +54,52 @@ __device__ __forceinline__ uint32_t shl_clamp(uint32_t a, uint32_t b) {
 // Low 16 bits of remix32(hi ^ lo) of a 64-bit candidate.
 __device__ __forceinline__ uint32_t hash16(uint64_t v) { return remix32(uint32_t(v >> 32) ^ uint32_t(v)) & 0xFFFFu; }
 
-// acc[s] += sum over keys of the part index p(k, x) of candidate x = bu + lane + 32 s, where
-// bu is the warp-uniform window base. The 64-bit key + base sum is formed once per key.
-// When its low 16 bits cannot overflow within the window (all but ~S*32 / 2^16 of the
-// keys), every candidate differs from it only in bits 0..15, so remix32's first xor-shift
-// term (hi ^ hi >> 16 ^ lo >> 16) is one per-key constant K and a candidate costs a 32-bit
-// add and an xor before the two multiply rounds; other keys take the plain 64-bit form.
-// hash16 << 16 is formed as (z << 16) ^ (z & 0xFFFF0000). With b = hash16 << 16, the part
-// index ((hash16 * m) >> 16) / SPLIT of a full node (m = fan * SPLIT) is umulhi(b, fan); for
-// any other node it is umulhi(b, mult) >> 28 with mult = ceil(m * 2^28 / SPLIT) (< 2^32 as
-// m < 16 * SPLIT; exact for every 16-bit hash, every leaf size and node size, checked
-// exhaustively). The multiply-high runs on the FMA pipe, beside the ALU work of the hash. An
-// exactly balanced split has sum_j j * size_j, so this sum is a necessary condition.
+// remix32 without its final xor-shift: hash16 = (z ^ z >> 16) & 0xFFFF = lo16(z) ^ hi16(z).
+__device__ __forceinline__ uint32_t remix32_core(uint32_t z) {
+    z ^= z >> 16;
+    z *= 0x85ebca6bu;
+    z ^= z >> 13;
+    return z * 0xc2b2ae35u;
+}
+
+// Starting value of a full node's part-index accumulator: the bits of the fp32 2^23.
+constexpr uint32_t kAccF0 = 0x4B000000u;
+
+// Adds the part index of one candidate, given z = remix32_core of its key + seed, to acc.
+// Full node (m = fan * SPLIT): the part index ((hash16 * m) >> 16) / SPLIT is
+// p = floor(hash16 * fan / 2^16). The bits kAccF0 | hash16 are the fp32 F = 2^23 + hash16, and
+// F * (fan / 2^16) = 128 fan + hash16 * fan / 2^16, so with acc an integer-valued fp32 in
+// [2^23, 2^24), where the spacing of fp32 values is 1, one fused multiply-add rounded toward
+// minus infinity gives exactly acc + 128 fan + p: acc counts 2^23 + 128 fan m + sum p after m
+// keys, which stays below 2^24 for every node (128 fan m < 2^23). The add runs on the FP32
+// pipes, beside the integer hash. Other nodes: with b = hash16 << 16, p = umulhi(b, mult) >> 28
+// for mult = ceil(m * 2^28 / SPLIT) (< 2^32 as m < 16 * SPLIT; exact for every 16-bit hash,
+// leaf size and node size, checked exhaustively).
+template <bool FULL>
+__device__ __forceinline__ void add_part(uint32_t z, uint32_t mult, float cf, uint32_t &acc) {
+    if (FULL) {
+        const uint32_t f = (z & 0xFFFFu) ^ __funnelshift_r(z, kAccF0 >> 16, 16);
+        acc = __float_as_uint(__fmaf_rd(__uint_as_float(f), cf, __uint_as_float(acc)));
+    } else {
+        acc += __umulhi((z << 16) ^ (z & 0xFFFF0000u), mult) >> 28;
+    }
+}
+
+// acc[s] += the part index p(k, x) of candidate x = bu + lane + 32 s, summed over keys (in
+// add_part's form), where bu is the warp-uniform window base; mult is fan for a full node. The
+// 64-bit key + base sum is formed once per key. When its low 16 bits cannot overflow within
+// the window (all but ~S*32 / 2^16 of the keys), every candidate differs from it only in bits
+// 0..15, so remix32's first xor-shift term (hi ^ hi >> 16 ^ lo >> 16) is one per-key constant
+// K and a candidate costs a 32-bit add and an xor before the two multiply rounds; other keys
+// take the plain 64-bit form. An exactly balanced split has sum_j j * size_j, so this sum is
+// a necessary condition.
 template <int S, bool FULL>
 __device__ __forceinline__ void moment_sums(const uint64_t *sk, uint32_t m, uint64_t bu, uint32_t mult,
                                             uint32_t *acc) {
     constexpr uint32_t kSpan = 32u * S;
     static_assert(kSpan <= 0x10000u, "window wider than the hoisting allows");
     const uint32_t lane = threadIdx.x & 31;
+    const float cf = (float)mult * 0x1p-16f;
 #pragma unroll 4
     for (uint32_t i = 0; i < m; ++i) {
         const uint64_t tu = sk[i] + bu;
@@ -79,8 +107,8 @@ __device__ __forceinline__ void moment_sums(const uint64_t *sk, uint32_t m, uint
         if ((lo0 & 0xFFFFu) > 0x10000u - kSpan) {
 #pragma unroll
             for (int s = 0; s < S; ++s) {
-                const uint32_t r = __umulhi(hash16(tu + lane + 32u * s) << 16, mult);
-                acc[s] += FULL ? r : r >> 28;
+                const uint64_t v = tu + lane + 32u * s;
+                add_part<FULL>(remix32_core(uint32_t(v >> 32) ^ uint32_t(v)), mult, cf, acc[s]);
             }
         } else {
             const uint32_t K = hi ^ (hi >> 16) ^ (lo0 >> 16);
@@ -90,9 +118,7 @@ __device__ __forceinline__ void moment_sums(const uint64_t *sk, uint32_t m, uint
                 uint32_t z = (l0 + 32u * s) ^ K;
                 z *= 0x85ebca6bu;
                 z ^= z >> 13;
-                z *= 0xc2b2ae35u;
-                const uint32_t r = __umulhi((z << 16) ^ (z & 0xFFFF0000u), mult);
-                acc[s] += FULL ? r : r >> 28;
+                add_part<FULL>(z * 0xc2b2ae35u, mult, cf, acc[s]);
             }
         }
     }
@@ -266,6 +292,7 @@ struct AggrCfg {
     static constexpr bool WIDE = MAXF > 4;
     static constexpr uint64_t SEED_INDEX = STAGE == kStageUpper ? 17 : 18;
     static constexpr uint32_t WARP_WORDS = MAXM + QCAP;  // keys + candidate queue
+    static_assert(129u * MAXF * MAXM < (1u << 23), "full-node accumulator leaves [2^23, 2^24)");
 };
 
 __device__ __forceinline__ uint64_t warp_min_u64(uint64_t v) {
@@ -374,9 +401,10 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
                 if (j < 4) tlo |= t << (8 * j);
                 else thi |= t << (8 * (j - 4));
             }
-            // phase A target: sum_j j * size_j; part-index multiplier of non-full nodes
+            // phase A target: sum_j j * size_j, in add_part's form; part-index multiplier of
+            // non-full nodes
             mult = (uint32_t)((((uint64_t)m << 28) + C::SPLIT - 1) / C::SPLIT);
-            t1 = 0;
+            t1 = full ? kAccF0 + 128u * fan * m : 0u;
             for (uint32_t j = 1; j < fan; ++j) t1 += j * (j + 1 < fan ? C::SPLIT : m - (fan - 1) * C::SPLIT);
             budget = budget_for(c, m);
             qn = 0;
@@ -399,7 +427,7 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
         // phase A: part-index sums for S seeds per lane (seeds x0 + lane + 32 s)
         uint32_t cnt[S];
 #pragma unroll
-        for (int s = 0; s < S; ++s) cnt[s] = 0;
+        for (int s = 0; s < S; ++s) cnt[s] = full ? kAccF0 : 0u;
         // The keys go in chunks; after each chunk the window is abandoned if the node's best
         // seed has dropped to x0 or below (another warp succeeded below this window), since
         // then none of its candidates can lower the minimum.
@@ -869,7 +897,7 @@ __global__ void __launch_bounds__(kThreads) k_probe(unsigned long long *sink) {
     __syncthreads();
     uint32_t cnt[kProbeSeeds];
 #pragma unroll
-    for (int s = 0; s < kProbeSeeds; ++s) cnt[s] = 0;
+    for (int s = 0; s < kProbeSeeds; ++s) cnt[s] = kAccF0;
     uint64_t bu = start_seed(17) + (blockIdx.x * (uint64_t)kWarpsPerCta + (threadIdx.x >> 5)) * 32 * kProbeSeeds;
     for (int it = 0; it < kProbeIters; ++it) {
         moment_sums<kProbeSeeds, true>(sk, kProbeKeys, bu, 7u, cnt);
