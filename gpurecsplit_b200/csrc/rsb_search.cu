@@ -526,10 +526,36 @@ __device__ __forceinline__ uint32_t rotl_leaf(uint32_t v, uint32_t r) {
     return ((v << r) | (v >> (LEAF - r))) & full;
 }
 
-// Left masks of the S bases x0 + lane + 32 s of a rotation-leaf window (bu = SEED + x0*LEAF),
-// with the same per-key hoisting as moment_sums (the window spans 32*S*LEAF seeds). The bit
-// of a key is remap16(key + seed, LEAF) = umulhi(hash16 << 16, LEAF), a multiply-high on
-// the FMA pipe beside the hash's ALU work.
+// Adds the bit of one key, given z = remix32_core of key + seed, to a left-mask sum. The
+// bit index p = remap16 = floor(hash16 * LEAF / 2^16) comes from one fp32 fused multiply-add
+// rounded toward minus infinity, as in add_part: F = 2^23 + hash16 (bits kAccF0 | hash16)
+// times LEAF / 2^16 plus 2^23 - 128 LEAF is exactly 2^23 + hash16 * LEAF / 2^16, which rounds
+// down to the integer-valued fp32 2^23 + p, whose bits are kAccF0 + p. Times 2^23 plus
+// 127 << 23 (mod 2^32) these bits become (127 + p) << 23, the fp32 2^p, which is added to the
+// fp32 sum acc. Only the final integer add runs on the ALU pipe beside the hash.
+template <int LEAF>
+__device__ __forceinline__ void add_bit(uint32_t z, uint32_t &acc) {
+    constexpr float kScale = (float)LEAF * 0x1p-16f, kBias = 0x1p23f - 128.0f * LEAF;
+    const uint32_t f = (z & 0xFFFFu) ^ __funnelshift_r(z, kAccF0 >> 16, 16);
+    const uint32_t t = __float_as_uint(__fmaf_rd(__uint_as_float(f), kScale, kBias));
+    acc = __float_as_uint(__fadd_rn(__uint_as_float(acc), __uint_as_float(t * (1u << 23) + (127u << 23))));
+}
+
+// The left mask of a sum formed by add_bit over nl keys, or ~0u when two keys share a bit.
+// Without a shared bit the terms are distinct powers of two below 2^LEAF <= 2^24, every
+// partial sum is an integer below 2^24 and exact in fp32, and the sum is the mask with nl
+// bits set. With one, either every partial sum stays below 2^24 (exact), and the carry leaves
+// fewer than nl bits set, or the sum reaches 2^24 or more, out of the mask's range.
+template <int LEAF>
+__device__ __forceinline__ uint32_t left_mask_of(uint32_t acc, uint32_t nl) {
+    static_assert(LEAF <= 24, "left-mask sums are exact below 2^24 only");
+    const uint32_t mk = __float2uint_rz(__uint_as_float(acc));
+    return (mk >> LEAF) == 0 && __popc(mk) == (int)nl ? mk : ~0u;
+}
+
+// Left-mask sums (add_bit) of the S bases x0 + lane + 32 s of a rotation-leaf window
+// (bu = SEED + x0*LEAF), with the same per-key hoisting as moment_sums (the window spans
+// 32*S*LEAF seeds).
 template <int LEAF, int S>
 __device__ __forceinline__ void left_masks(const uint64_t *sk, uint32_t nl, uint64_t bu, uint32_t *ml) {
     constexpr uint32_t kSpan = 32u * S * LEAF;
@@ -541,8 +567,10 @@ __device__ __forceinline__ void left_masks(const uint64_t *sk, uint32_t nl, uint
         const uint32_t lo0 = (uint32_t)tu, hi = (uint32_t)(tu >> 32);
         if ((lo0 & 0xFFFFu) > 0x10000u - kSpan) {
 #pragma unroll
-            for (int s = 0; s < S; ++s)
-                ml[s] |= 1u << __umulhi(hash16(tu + (lane + 32u * s) * LEAF) << 16, (uint32_t)LEAF);
+            for (int s = 0; s < S; ++s) {
+                const uint64_t v = tu + (lane + 32u * s) * LEAF;
+                add_bit<LEAF>(remix32_core(uint32_t(v >> 32) ^ uint32_t(v)), ml[s]);
+            }
         } else {
             const uint32_t K = hi ^ (hi >> 16) ^ (lo0 >> 16);
             const uint32_t l0 = lo0 + lane * LEAF;
@@ -551,8 +579,7 @@ __device__ __forceinline__ void left_masks(const uint64_t *sk, uint32_t nl, uint
                 uint32_t z = (l0 + 32u * s * LEAF) ^ K;
                 z *= 0x85ebca6bu;
                 z ^= z >> 13;
-                z *= 0xc2b2ae35u;
-                ml[s] |= 1u << __umulhi((z << 16) ^ (z & 0xFFFF0000u), (uint32_t)LEAF);
+                add_bit<LEAF>(z * 0xc2b2ae35u, ml[s]);
             }
         }
     }
@@ -665,7 +692,7 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
         }
         uint32_t off = 0xFFFFFFFFu;
         if (ROT) {
-            // phase A: left masks of S bases per lane; queue the collision-free ones
+            // phase A: left-mask sums of S bases per lane; queue the collision-free ones
             const unsigned below = (1u << lane) - 1;
             uint32_t ml[S];
 #pragma unroll
@@ -674,11 +701,12 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
 #pragma unroll
             for (int s = 0; s < S; ++s) {
                 const uint64_t b = x0 + lane + 32u * s;
-                const bool pass = __popc(ml[s]) == (int)nl;
+                const uint32_t mk = left_mask_of<LEAF>(ml[s], nl);
+                const bool pass = mk != ~0u;
                 const unsigned bal = __ballot_sync(0xffffffffu, pass);
                 if (pass) {
                     qb[qn + __popc(bal & below)] = b;
-                    qm[qn + __popc(bal & below)] = ml[s];
+                    qm[qn + __popc(bal & below)] = mk;
                 }
                 qn += __popc(bal);
             }
