@@ -85,43 +85,67 @@ __device__ __forceinline__ void add_part(uint32_t z, uint32_t mult, float cf, ui
     }
 }
 
-// acc[s] += the part index p(k, x) of candidate x = bu + lane + 32 s, summed over keys (in
-// add_part's form), where bu is the warp-uniform window base; mult is fan for a full node. The
-// 64-bit key + base sum is formed once per key. When its low 16 bits cannot overflow within
-// the window (all but ~S*32 / 2^16 of the keys), every candidate differs from it only in bits
-// 0..15, so remix32's first xor-shift term (hi ^ hi >> 16 ^ lo >> 16) is one per-key constant
-// K and a candidate costs a 32-bit add and an xor before the two multiply rounds; other keys
-// take the plain 64-bit form. An exactly balanced split has sum_j j * size_j, so this sum is
-// a necessary condition.
+// Keys of an aggregation node per phase-A pass: after each chunk the window is abandoned if
+// the node's best seed has dropped to its first candidate.
+constexpr uint32_t kAbortChunk = 64;
+
+// acc[s] += the part index p(k, x) of candidate x = bu + lane + 32 s, summed over the len <=
+// kAbortChunk keys sk[0, len) (in add_part's form), where bu is the warp-uniform window base;
+// mult is fan for a full node. When the low 16 bits of key + bu cannot overflow within the
+// window (all but ~S*32 / 2^16 of the keys), every candidate differs from key + bu only in
+// bits 0..15: with lo = low word, hi = high word and L = lo & 0xFFFF, remix32's input
+// (hi ^ lo) ^ (hi ^ lo) >> 16 is (L + j) ^ K' for the candidate bu + j, where
+// K' = hi ^ hi >> 16 ^ lo >> 16 ^ (lo & 0xFFFF0000) is one per-key constant. The warp first
+// computes (K', L) of every such key of the chunk, one key per lane, into pk[0, nf) (shared
+// memory), and the indexes of the other keys into pk[kAbortChunk - ns, kAbortChunk); then a
+// candidate costs a 32-bit add and an xor before the two multiply rounds, and the few other
+// keys take the plain 64-bit form. An exactly balanced split has sum_j j * size_j, so this
+// sum is a necessary condition.
 template <int S, bool FULL>
-__device__ __forceinline__ void moment_sums(const uint64_t *sk, uint32_t m, uint64_t bu, uint32_t mult,
-                                            uint32_t *acc) {
+__device__ __forceinline__ void moment_sums(const uint64_t *sk, uint32_t len, uint64_t bu, uint32_t mult,
+                                            uint2 *pk, uint32_t *acc) {
     constexpr uint32_t kSpan = 32u * S;
     static_assert(kSpan <= 0x10000u, "window wider than the hoisting allows");
     const uint32_t lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1;
     const float cf = (float)mult * 0x1p-16f;
+    uint32_t nf = 0, ns = 0;
+    for (uint32_t c0 = 0; c0 < len; c0 += 32) {
+        const uint32_t i = c0 + lane;
+        const bool valid = i < len;
+        const uint64_t tu = (valid ? sk[i] : 0) + bu;
+        const uint32_t lo = (uint32_t)tu, hi = (uint32_t)(tu >> 32);
+        const bool fast = (lo & 0xFFFFu) <= 0x10000u - kSpan;
+        const unsigned bf = __ballot_sync(0xffffffffu, valid && fast);
+        const unsigned bs = __ballot_sync(0xffffffffu, valid && !fast);
+        if (valid && fast)
+            pk[nf + __popc(bf & below)] = make_uint2(hi ^ (hi >> 16) ^ (lo >> 16) ^ (lo & 0xFFFF0000u), lo & 0xFFFFu);
+        if (valid && !fast) pk[kAbortChunk - 1 - ns - __popc(bs & below)].x = i;
+        nf += __popc(bf);
+        ns += __popc(bs);
+    }
+    __syncwarp();
 #pragma unroll 4
-    for (uint32_t i = 0; i < m; ++i) {
-        const uint64_t tu = sk[i] + bu;
-        const uint32_t lo0 = (uint32_t)tu, hi = (uint32_t)(tu >> 32);
-        if ((lo0 & 0xFFFFu) > 0x10000u - kSpan) {
+    for (uint32_t j = 0; j < nf; ++j) {
+        const uint2 e = pk[j];
+        const uint32_t l0 = e.y + lane;
 #pragma unroll
-            for (int s = 0; s < S; ++s) {
-                const uint64_t v = tu + lane + 32u * s;
-                add_part<FULL>(remix32_core(uint32_t(v >> 32) ^ uint32_t(v)), mult, cf, acc[s]);
-            }
-        } else {
-            const uint32_t K = hi ^ (hi >> 16) ^ (lo0 >> 16);
-            const uint32_t l0 = lo0 + lane;
-#pragma unroll
-            for (int s = 0; s < S; ++s) {
-                uint32_t z = (l0 + 32u * s) ^ K;
-                z *= 0x85ebca6bu;
-                z ^= z >> 13;
-                add_part<FULL>(z * 0xc2b2ae35u, mult, cf, acc[s]);
-            }
+        for (int s = 0; s < S; ++s) {
+            uint32_t z = (l0 + 32u * s) ^ e.x;
+            z *= 0x85ebca6bu;
+            z ^= z >> 13;
+            add_part<FULL>(z * 0xc2b2ae35u, mult, cf, acc[s]);
         }
     }
+    for (uint32_t j = 0; j < ns; ++j) {
+        const uint64_t tu = sk[pk[kAbortChunk - 1 - j].x] + bu;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const uint64_t v = tu + lane + 32u * s;
+            add_part<FULL>(remix32_core(uint32_t(v >> 32) ^ uint32_t(v)), mult, cf, acc[s]);
+        }
+    }
+    __syncwarp();  // pk is rewritten by the next chunk
 }
 
 __device__ __forceinline__ uint64_t budget_for(const SearchCtx &c, uint32_t m) {
@@ -273,7 +297,6 @@ __global__ void __launch_bounds__(kHigherThreads) k_search_higher(SearchCtx c, i
 // count. A warp drains its queue before it leaves a node, so every seed below the node's
 // final best is still fully checked and the minimum is unchanged.
 // ---------------------------------------------------------------------------------------
-constexpr uint32_t kAbortChunk = 64;  // keys between checks of the node's best seed
 
 // Candidates per lane of a window, by leaf size (measured on one B200): 12 amortise the
 // per-key work better where nodes need thousands of candidates or more (l = 16: 253 -> 247
@@ -291,7 +314,7 @@ struct AggrCfg {
     static constexpr uint32_t MAXF = (MAXM + SPLIT - 1) / SPLIT;
     static constexpr bool WIDE = MAXF > 4;
     static constexpr uint64_t SEED_INDEX = STAGE == kStageUpper ? 17 : 18;
-    static constexpr uint32_t WARP_WORDS = MAXM + QCAP;  // keys + candidate queue
+    static constexpr uint32_t WARP_WORDS = MAXM + QCAP + kAbortChunk;  // keys, candidate queue, key terms
     static_assert(129u * MAXF * MAXM < (1u << 23), "full-node accumulator leaves [2^23, 2^24)");
 };
 
@@ -361,6 +384,7 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint64_t *sk = smem + warp * C::WARP_WORDS;
     uint64_t *q = sk + C::MAXM;
+    uint2 *pk = reinterpret_cast<uint2 *>(q + C::QCAP);
     const unsigned below = (1u << lane) - 1;
     const uint32_t gw = blockIdx.x * kWarpsPerCta + warp;
     const uint32_t count = c.stage_info[STAGE];
@@ -434,8 +458,8 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
         bool abandoned = false;
         for (uint32_t i0 = 0; i0 < m; i0 += kAbortChunk) {
             const uint32_t len = min(kAbortChunk, m - i0);
-            if (full) moment_sums<S, true>(sk + i0, len, seed + x0, fan, cnt);
-            else moment_sums<S, false>(sk + i0, len, seed + x0, mult, cnt);
+            if (full) moment_sums<S, true>(sk + i0, len, seed + x0, fan, pk, cnt);
+            else moment_sums<S, false>(sk + i0, len, seed + x0, mult, pk, cnt);
             if (i0 + len < m) {
                 uint64_t b = 0;
                 if (lane == 0) b = vload64(&c.nodes.seed[node]);
@@ -912,15 +936,16 @@ void search_leaves(const SearchCtx &c, int stage, cudaStream_t st) {
 // ---- eval-rate probe ------------------------------------------------------------------
 // The cheapest complete candidate evaluation of any search (key + seed, remix32, 16-bit
 // remap to a part index, sum) in the exact form of the aggregation filter (moment_sums on a
-// full node: keys broadcast from shared memory, 12 candidates per lane, unrolled key loop),
-// run at full occupancy with no scheduling, no queues and no reductions: the integer
-// ceiling for remixAndRemap32 evaluations on this device.
+// full node in chunks of kAbortChunk keys: per-key terms in shared memory, 12 candidates per
+// lane, unrolled key loop), run at full occupancy with no scheduling, no queues and no
+// reductions: the ceiling for remixAndRemap32 evaluations on this device.
 namespace {
-constexpr int kProbeKeys = 128;
+constexpr uint32_t kProbeKeys = 128;
 constexpr int kProbeIters = 32;
 constexpr int kProbeSeeds = 12;
 __global__ void __launch_bounds__(kThreads) k_probe(unsigned long long *sink) {
     __shared__ uint64_t sk[kProbeKeys];
+    __shared__ uint2 pk[kWarpsPerCta][kAbortChunk];
     for (int i = threadIdx.x; i < kProbeKeys; i += kThreads) sk[i] = start_seed(i % 20) * (2 * i + 1);
     __syncthreads();
     uint32_t cnt[kProbeSeeds];
@@ -928,7 +953,9 @@ __global__ void __launch_bounds__(kThreads) k_probe(unsigned long long *sink) {
     for (int s = 0; s < kProbeSeeds; ++s) cnt[s] = kAccF0;
     uint64_t bu = start_seed(17) + (blockIdx.x * (uint64_t)kWarpsPerCta + (threadIdx.x >> 5)) * 32 * kProbeSeeds;
     for (int it = 0; it < kProbeIters; ++it) {
-        moment_sums<kProbeSeeds, true>(sk, kProbeKeys, bu, 7u, cnt);
+#pragma unroll 1
+        for (uint32_t i0 = 0; i0 < kProbeKeys; i0 += kAbortChunk)
+            moment_sums<kProbeSeeds, true>(sk + i0, kAbortChunk, bu, 7u, pk[threadIdx.x >> 5], cnt);
         bu += 1ull << 32;
     }
     uint32_t tot = 0;
