@@ -578,35 +578,47 @@ __device__ __forceinline__ uint32_t left_mask_of(uint32_t acc, uint32_t nl) {
 }
 
 // Left-mask sums (add_bit) of the S bases x0 + lane + 32 s of a rotation-leaf window
-// (bu = SEED + x0*LEAF), with the same per-key hoisting as moment_sums (the window spans
-// 32*S*LEAF seeds).
+// (bu = SEED + x0*LEAF) over the nl < 32 left keys sk[0, nl), with moment_sums' per-key terms:
+// the window spans 32*S*LEAF seeds, each key's (K', L) goes to pk[0, nf) and the indexes of
+// keys whose low half can overflow within the window to pk[LEAF - ns, LEAF).
 template <int LEAF, int S>
-__device__ __forceinline__ void left_masks(const uint64_t *sk, uint32_t nl, uint64_t bu, uint32_t *ml) {
+__device__ __forceinline__ void left_masks(const uint64_t *sk, uint32_t nl, uint64_t bu, uint2 *pk, uint32_t *ml) {
     constexpr uint32_t kSpan = 32u * S * LEAF;
     static_assert(kSpan <= 0x10000u, "window wider than the hoisting allows");
     const uint32_t lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1;
+    const bool valid = lane < nl;
+    const uint64_t tu = (valid ? sk[lane] : 0) + bu;
+    const uint32_t lo = (uint32_t)tu, hi = (uint32_t)(tu >> 32);
+    const bool fast = (lo & 0xFFFFu) <= 0x10000u - kSpan;
+    const unsigned bf = __ballot_sync(0xffffffffu, valid && fast);
+    const unsigned bs = __ballot_sync(0xffffffffu, valid && !fast);
+    if (valid && fast)
+        pk[__popc(bf & below)] = make_uint2(hi ^ (hi >> 16) ^ (lo >> 16) ^ (lo & 0xFFFF0000u), lo & 0xFFFFu);
+    if (valid && !fast) pk[LEAF - 1 - __popc(bs & below)].x = lane;
+    const uint32_t nf = __popc(bf), ns = __popc(bs);
+    __syncwarp();
 #pragma unroll 2
-    for (uint32_t i = 0; i < nl; ++i) {
-        const uint64_t tu = sk[i] + bu;
-        const uint32_t lo0 = (uint32_t)tu, hi = (uint32_t)(tu >> 32);
-        if ((lo0 & 0xFFFFu) > 0x10000u - kSpan) {
+    for (uint32_t i = 0; i < nf; ++i) {
+        const uint2 e = pk[i];
+        const uint32_t l0 = e.y + lane * LEAF;
 #pragma unroll
-            for (int s = 0; s < S; ++s) {
-                const uint64_t v = tu + (lane + 32u * s) * LEAF;
-                add_bit<LEAF>(remix32_core(uint32_t(v >> 32) ^ uint32_t(v)), ml[s]);
-            }
-        } else {
-            const uint32_t K = hi ^ (hi >> 16) ^ (lo0 >> 16);
-            const uint32_t l0 = lo0 + lane * LEAF;
-#pragma unroll
-            for (int s = 0; s < S; ++s) {
-                uint32_t z = (l0 + 32u * s * LEAF) ^ K;
-                z *= 0x85ebca6bu;
-                z ^= z >> 13;
-                add_bit<LEAF>(z * 0xc2b2ae35u, ml[s]);
-            }
+        for (int s = 0; s < S; ++s) {
+            uint32_t z = (l0 + 32u * s * LEAF) ^ e.x;
+            z *= 0x85ebca6bu;
+            z ^= z >> 13;
+            add_bit<LEAF>(z * 0xc2b2ae35u, ml[s]);
         }
     }
+    for (uint32_t i = 0; i < ns; ++i) {
+        const uint64_t t = sk[pk[LEAF - 1 - i].x] + bu;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const uint64_t v = t + (lane + 32u * s) * LEAF;
+            add_bit<LEAF>(remix32_core(uint32_t(v >> 32) ^ uint32_t(v)), ml[s]);
+        }
+    }
+    __syncwarp();  // pk is rewritten by the next window
 }
 
 // Phase B of rotation leaves: each lane takes one queued (base, left mask).
@@ -646,6 +658,7 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
     constexpr int S = kLeafSeedsPerLane;
     constexpr uint32_t W = 32 * S;
     __shared__ uint64_t skeys[kWarpsPerCta][LEAF];
+    __shared__ uint2 s_pk[ROT ? kWarpsPerCta : 1][ROT ? LEAF : 1];
     __shared__ uint64_t s_qb[ROT ? kWarpsPerCta : 1][ROT ? kLeafQueueCap : 1];
     __shared__ uint32_t s_qm[ROT ? kWarpsPerCta : 1][ROT ? kLeafQueueCap : 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -721,7 +734,7 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
             uint32_t ml[S];
 #pragma unroll
             for (int s = 0; s < S; ++s) ml[s] = 0;
-            left_masks<LEAF, S>(sk, nl, seed + x0 * LEAF, ml);
+            left_masks<LEAF, S>(sk, nl, seed + x0 * LEAF, s_pk[ROT ? warp : 0], ml);
 #pragma unroll
             for (int s = 0; s < S; ++s) {
                 const uint64_t b = x0 + lane + 32u * s;
