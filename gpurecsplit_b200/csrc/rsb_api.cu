@@ -162,15 +162,6 @@ rsb_status get_device_tables(rsb_engine *e, const LeafTables &t, uint32_t leaf, 
     return RSB_OK;
 }
 
-bool is_device_pointer(const void *p) {
-    cudaPointerAttributes a{};
-    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
-}
-
 float elapsed(cudaEvent_t a, cudaEvent_t b) {
     float ms = 0;
     if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
