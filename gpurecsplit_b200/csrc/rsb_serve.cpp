@@ -41,7 +41,11 @@ namespace {
 using Clock = std::chrono::steady_clock;
 
 constexpr double kSmallMs = 20.0;
-constexpr uint32_t kLargeLaneOccupancy = 75;
+// 67: with 16K-register search CTAs (256 threads x 64 registers) a large lane at 75 % holds 3
+// of an SM's 4 CTA slots of registers and small builds slowed down several-fold (mixed-load
+// p50 139 ms); at 67 % it holds 2 and the p50 is 28 ms at the same capacity (measured on one
+// B200 with the serving benchmark).
+constexpr uint32_t kLargeLaneOccupancy = 67;
 
 // Device ns per key of a build by leaf size, interpolated geometrically between rates
 // measured on one B200 (l = 8: 2, 12: 5, 16: 250, 24: 1e5 ns/key); used only to route
