@@ -289,8 +289,9 @@ __global__ void __launch_bounds__(kHigherThreads) k_search_higher(SearchCtx c, i
 // ---------------------------------------------------------------------------------------
 //
 // Two-phase evaluation. A seed can only split a node exactly if the sum over its keys of
-// the part index equals sum_j j * size_j — a necessary condition that costs one or two
-// multiply-highs and an add per key (moment_sums) instead of a packed part count, and that
+// the part index equals sum_j j * size_j — a necessary condition that costs one fused
+// multiply-add per key on a full node (two integer ops more on other nodes; moment_sums and
+// add_part) instead of a packed part count, and that
 // about 1 / (2.5 * sqrt(m * var(p))) of the seeds pass (1.9 % at m = 112, fanout 7).
 // Phase A applies it to every seed of a window (8 or 12 per lane); the survivors go to a per-warp
 // queue in shared memory, and phase B gives each lane one queued seed for the exact part
