@@ -13,17 +13,19 @@ keys (splitmix64, seed 42 + rank) with leaf size 16, bucket size 2000 and rotati
   roofline  the dominant search kernel's algorithmic evaluation rate (sum over its nodes
           of candidates x node size / its device time) against the device's measured
           remixAndRemap32 evaluation ceiling (rsb_probe_eval_rate)
-  cpu_baseline  SIMDRecSplit restated on all host cores (the CPU oracle with its seed
-          searches in AVX-512 intrinsics; the scalar oracle on CPUs without AVX-512) on a
-          bounded sample of the same workload
+  cpu_baseline  the reference's own SIMDRecSplit (compiled from its sources into
+          oracle/_ref) on all host cores, on one contiguous fifth of the workload's buckets
+  c1, c3, c4_batch, c5_serve  the other configurations (1M string keys l=8 b=100; 200k keys
+          l=24 b=2000; 1000 batched sets l=12 b=1000; the serving loop), each with its own
+          clock record, timing and parity check (single GPU only)
 
-`--impl reference` times only that CPU implementation of the path (the reference's own
-SIMDRecSplit cannot be compiled here: its submodules are absent).
+`--impl reference` times only the CPU build (the reference's SIMDRecSplit from oracle/_ref;
+without it, this project's AVX-512 restatement): step i builds the i-th of `steps`
+contiguous bucket ranges, so the timed steps together build the whole workload once.
 
 Other modes (one JSON line each): `--mode batch` (many key sets in one pipeline vs
 back-to-back plain builds), `--mode serve` (continuous batching of string requests),
-`--mode c1` (1M printable string keys, l=8, b=100) and `--mode c3` (200k u64 keys, l=24,
-b=2000).
+`--mode c1` and `--mode c3`.
 
 Multi-GPU (torchrun): every rank builds its own 5M-key set (weak scaling, no data-path
 collective); the step time is the max over ranks.
@@ -147,57 +149,133 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------------------
-# CPU side (oracle) — the timed CPU baseline and the reference arm
+# CPU side — the reference's own SIMDRecSplit (oracle/_ref) on bucket ranges of the workload
 # ---------------------------------------------------------------------------------------
-def cpu_sample(buckets: int, seed: int = SEED):
-    """Keys of a bounded sample with the bench workload's shape: `buckets` buckets of b=2000."""
-    import oracle
-    n = buckets * BUCKET
-    keys = oracle.hash_u64(splitmix64_keys(seed, n))
-    return keys, n
+class CpuWorkload:
+    """The bench workload (n keys, l=16, b=2000) hashed to 128 bits and grouped by bucket,
+    for timing CPU builds on contiguous bucket ranges.
+
+    A range [lo, hi) of the workload's buckets is built as its own function: the keys keep
+    their second halves (which alone decide every seed) and their bucket sizes, and their first
+    halves are replaced by the smallest value that remap128 (support/common.hpp:273-280) maps
+    to the same bucket of an (hi - lo)-bucket function, whose bucket size is chosen so that it
+    has exactly hi - lo buckets. So a range build runs the reference's complete construction
+    (sort, partition, every seed search, Rice and Elias-Fano encoding) over exactly the seed
+    searches of those buckets in the full build, and ranges that cover the workload cover its
+    search work once.
+    """
+
+    def __init__(self, n: int = N_KEYS, seed: int = SEED):
+        import oracle
+        keys = oracle.hash_u64(splitmix64_keys(seed, n))
+        self.n = n
+        self.nb = (n + BUCKET - 1) // BUCKET
+        first = keys[:, 0]
+        nb = np.uint64(self.nb)
+        hi = first >> np.uint64(32)
+        lo = first & np.uint64(0xFFFFFFFF)
+        bucket = (hi * nb + ((lo * nb) >> np.uint64(32))) >> np.uint64(32)  # (first * nb) >> 64
+        order = np.argsort(bucket, kind="stable")
+        self.second = np.ascontiguousarray(keys[order, 1])
+        self.start = np.searchsorted(bucket[order], np.arange(self.nb + 1, dtype=np.uint64)).astype(np.int64)
+
+    def range_keys(self, lo: int, hi: int):
+        """(keys128, bucket size) of the function over buckets [lo, hi)."""
+        nb = hi - lo
+        a, z = int(self.start[lo]), int(self.start[hi])
+        n = z - a
+        b = max(1, -(-n // nb))
+        while -(-n // b) > nb:
+            b += 1
+        while b > 1 and -(-n // (b - 1)) == nb:
+            b -= 1
+        if max(1, -(-n // b)) != nb:
+            raise RuntimeError(f"no bucket size gives {nb} buckets for {n} keys")
+        out = np.empty((n, 2), dtype=np.uint64)
+        out[:, 1] = self.second[a:z]
+        sizes = np.diff(self.start[lo:hi + 1])
+        firsts = np.array([-(-(j << 64) // nb) for j in range(nb)], dtype=np.uint64)
+        out[:, 0] = np.repeat(firsts, sizes)
+        return out, b
+
+    def ranges(self, parts: int):
+        """`parts` contiguous bucket ranges covering every bucket once."""
+        return [(self.nb * i // parts, self.nb * (i + 1) // parts) for i in range(parts)]
 
 
-def time_cpu_oracle(buckets: int, threads: int) -> dict:
-    """SIMDRecSplit restated (the oracle with AVX-512 search loops) when the CPU has AVX-512,
-    else the scalar oracle, on `buckets` buckets of the workload with `threads` threads."""
+def cpu_impl():
+    """(build function, kind, description) of the CPU build that is timed."""
     import oracle
-    simd = oracle.simd_supported()
-    keys, n = cpu_sample(buckets)
-    t0 = time.perf_counter()
-    res = oracle.build_mphf(keys, LEAF, BUCKET, True, threads=threads, simd=simd)
-    dt = time.perf_counter() - t0
-    impl = ("SIMDRecSplit restated: oracle with AVX-512 search loops (16 seeds per 512-bit vector)" if simd
-            else "scalar oracle (this CPU lacks AVX-512)")
-    return {"value": dt * 1e9 / n, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{buckets} buckets of b={BUCKET} ({n} keys, same key stream and l={LEAF}) out of the "
-                      f"{(N_KEYS + BUCKET - 1) // BUCKET}-bucket workload; {impl}, {threads} threads on "
-                      f"{oracle.cpu_model()}",
-            "seconds": dt, "bits_per_key": oracle.get_bits(res.bytes) / n}
+    oracle.build()
+    if oracle.ref_available():
+        return (lambda k, b, t: oracle.ref_build(k, LEAF, b, True, threads=t), "reference",
+                "the reference's own SIMDRecSplit (include/function/SIMDRecSplit.hpp) compiled from its sources "
+                "with AVX-512 (oracle/_ref)")
+    if oracle.simd_supported():
+        return (lambda k, b, t: oracle.build_mphf(k, LEAF, b, True, threads=t, simd=True).bytes, "port",
+                "SIMDRecSplit restated with AVX-512 search loops (oracle/_build/libsimdrs.so)")
+    return (lambda k, b, t: oracle.build_mphf(k, LEAF, b, True, threads=t).bytes, "port", "scalar oracle")
+
+
+def time_cpu_ranges(work: CpuWorkload, ranges, threads: int, build):
+    """Seconds and keys of one CPU build per bucket range."""
+    out = []
+    for lo, hi in ranges:
+        keys, b = work.range_keys(lo, hi)
+        t0 = time.perf_counter()
+        blob = build(keys, b, threads)
+        dt = time.perf_counter() - t0
+        assert blob.size > 0
+        out.append((dt, keys.shape[0]))
+    return out
+
+
+def cpu_baseline(args) -> dict:
+    """The CPU build timed on a bounded sample: one contiguous fifth of the workload's buckets
+    (about 1M keys, 10-30 s on the box's host cores), on all host cores."""
+    import oracle
+    build, kind, what = cpu_impl()
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    work = CpuWorkload(args.n)
+    parts = max(1, args.cpu_fraction)
+    lo, hi = work.ranges(parts)[parts // 2]
+    (secs, keys), = time_cpu_ranges(work, [(lo, hi)], threads, build)
+    return {"value": secs * 1e9 / keys, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"buckets [{lo}, {hi}) of the {work.nb}-bucket workload ({keys} keys, built as one function "
+                      f"with the same buckets and seed searches); {what}, {threads} threads on {oracle.cpu_model()}",
+            "seconds": secs}
 
 
 def run_reference(args, rank: int, world: int) -> None:
+    """The reference arm: the reference's own SIMDRecSplit on all host cores. Step i builds
+    buckets [i*nb/steps, (i+1)*nb/steps) of the workload, so the timed steps together build
+    the whole n=5M workload exactly once; warm-up steps build a 4-bucket range each."""
     if rank != 0:
         return
     import oracle
-    oracle.build()
-    threads = os.cpu_count() or 1
-    if args.ref_buckets is None:
-        args.ref_buckets = 96 if oracle.simd_supported() else 24
-    for _ in range(args.warmup):
-        time_cpu_oracle(args.ref_buckets, threads)
-    vals = [time_cpu_oracle(args.ref_buckets, threads) for _ in range(args.steps)]
-    v = statistics.mean(x["value"] for x in vals)
+    build, kind, what = cpu_impl()
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    work = CpuWorkload(args.n)
+    for w in range(args.warmup):
+        lo = (w * 37) % (work.nb - 4)
+        time_cpu_ranges(work, [(lo, lo + 4)], threads, build)
+    res = time_cpu_ranges(work, work.ranges(args.steps), threads, build)
+    secs = sum(r[0] for r in res)
+    keys = sum(r[1] for r in res)
+    v = secs * 1e9 / keys
+    sample = (f"{args.steps} steps of {work.nb // args.steps}-{-(-work.nb // args.steps)} contiguous buckets each, "
+              f"together all {work.nb} buckets ({keys} keys) of the workload once; {what}, {threads} threads on "
+              f"{oracle.cpu_model()}")
     line = {
         "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": statistics.mean(x["seconds"] for x in vals) * 1e3, "higher_is_better": False,
+        "ms_per_step": secs / args.steps * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": v / PUBLISHED_NS_PER_KEY, "dtype": "u64", "data": "synthetic",
         "impl": "reference",
-        "config": workload_config(N_KEYS, world) | {"cpu_sample_buckets": args.ref_buckets},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": vals[0]["sample"]},
+        "config": workload_config(args.n, world),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "SIMDRecSplit restated on the host cores (the oracle with AVX-512 search loops, or the scalar "
-                "oracle on CPUs without AVX-512); the reference itself cannot be built here (its sux, "
-                "vectorclass, gcem, ips2ra and SpookyV2 submodules are empty)",
+        "note": "CPU build on the host cores; the per-range bucket size keeps every range's buckets, and so its "
+                "seed searches, those of the full build (the first key halves are re-mapped to the range)",
     }
     print(json.dumps(line), flush=True)
 
@@ -267,7 +345,8 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         g = json.load(open(GOLDEN)).get("u64_n5M_l16_b2000")
         if g is not None:
             blob = last.serialize()
-            parity = {"sha256_equals_oracle": hashlib.sha256(blob).hexdigest() == g["sha256"],
+            parity = {"sha256_equals_reference": hashlib.sha256(blob).hexdigest() == g["ref_sha256"],
+                      "golden": "u64_n5M_l16_b2000 (the reference's SIMDRecSplit build of the same keys)",
                       "bits_per_key": last.get_bits() / n}
     bits_per_key = last.get_bits() / n
     last.close()
@@ -312,12 +391,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
             traffic = json.load(open(PROFILE_TRAFFIC)).get(str(dom))
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            import oracle
-            oracle.build()
-            if args.cpu_buckets is None:
-                args.cpu_buckets = 192 if oracle.simd_supported() else 48
-            cpu = time_cpu_oracle(args.cpu_buckets, os.cpu_count() or 1)
-            cpu.pop("seconds", None)
+            cpu = cpu_baseline(args)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
@@ -340,6 +414,15 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
                               for i, v in enumerate(ms_search) if v > 0.05},
             "step_ms": [round(x, 3) for x in step_ms],
         }
+        if world == 1 and not args.no_extras:
+            # The other configurations, each with its own clock record, parity and timing
+            # (one GPU; at N > 1 the line carries the headline only).
+            del keys_dev, flush
+            torch.cuda.empty_cache()
+            line["c1"] = measure_config("c1", engine, steps=5, warmup=3, e2e_steps=2)
+            line["c3"] = measure_config("c3", engine, steps=1, warmup=1, e2e_steps=1)
+            line["c4_batch"] = measure_batch(args.sets, engine)
+            line["c5_serve"] = measure_serve(args.requests, args.max_keys, args.hbm_budget, args.inflight, args.load)
         print(json.dumps(line), flush=True)
     engine.close()
     if dist is not None:
@@ -393,18 +476,22 @@ CONFIGS = {
 }
 
 
-def run_config(args) -> None:
+def measure_config(name: str, engine=None, steps: int = 5, warmup: int = 3, e2e_steps: int = 2) -> dict:
     """Device build time of one plain configuration (keys resident in HBM, L2 flushed before
-    every timed step), end-to-end time from host keys, and parity with the oracle digest."""
+    every timed step), end-to-end time from host keys, and parity with the committed digest of
+    the reference's build. Warm-up builds are of the same configuration; for l=24 (seconds per
+    build) a single one-bucket build of the same leaf size loads the kernels instead."""
     import ctypes
 
     import torch
     import gpurecsplit_b200 as rsb
 
-    kind, seed, n, leaf, b, golden = CONFIGS[args.mode]
+    kind, seed, n, leaf, b, golden = CONFIGS[name]
     torch.cuda.set_device(0)
     stream = torch.cuda.current_stream()
-    engine = rsb.Engine(0, stream.cuda_stream)
+    own = engine is None
+    if own:
+        engine = rsb.Engine(0, stream.cuda_stream)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     L = rsb.lib()
     if kind == "strings":
@@ -414,11 +501,11 @@ def run_config(args) -> None:
         host_keys = (data, offsets)
         flags = rsb.RSB_ROTATE | rsb.RSB_KEYS_ON_DEVICE | rsb.RSB_DEVICE_ONLY
 
-        def device_build():
+        def device_build(count=n):
             h = ctypes.c_void_p()
             rsb._check(L.rsb_build_strings(engine.handle, ctypes.c_void_p(d_data.data_ptr()),
-                                           ctypes.c_void_p(d_off.data_ptr()), n, b, leaf, flags, ctypes.byref(h)),
-                       "rsb_build_strings")
+                                           ctypes.c_void_p(d_off.data_ptr()), count, b, leaf, flags,
+                                           ctypes.byref(h)), "rsb_build_strings")
             return rsb.GPURecSplit(bucket_size=b, leaf_size=leaf, _handle=h)
         h2d = data.nbytes + offsets.nbytes
     else:
@@ -426,76 +513,85 @@ def run_config(args) -> None:
         d_keys = torch.from_numpy(keys.view(np.int64)).to("cuda")
         host_keys = keys
 
-        def device_build():
-            return rsb.GPURecSplit.from_device(d_keys.data_ptr(), n, b, leaf, key_type="u64", engine=engine,
+        def device_build(count=n):
+            return rsb.GPURecSplit.from_device(d_keys.data_ptr(), count, b, leaf, key_type="u64", engine=engine,
                                                device_only=True)
         h2d = keys.nbytes
     torch.cuda.synchronize()
-    for _ in range(args.warmup):
+    small_warmup = leaf >= 20
+    for _ in range(warmup):
         flush.zero_()
-        device_build().close()
+        device_build(min(n, b) if small_warmup else n).close()
     times, stats = [], None
-    with ClockSampler(0) as clocks:
-        for _ in range(args.steps):
-            flush.zero_()
-            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s.record(stream)
-            f = device_build()
-            e.record(stream)
-            e.synchronize()
-            times.append(s.elapsed_time(e))
-            stats = f.stats()
-            f.close()
-    e2e = []
     blob = None
-    for i in range(3):
-        flush.zero_()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        f = rsb.GPURecSplit(host_keys, bucket_size=b, leaf_size=leaf, key_type=kind, engine=engine)
-        blob = f.serialize()
-        if i > 0:
+    with ClockSampler(0) as clocks:
+        for _ in range(steps):
+            flush.zero_()
+            s0, e0 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            f = device_build()
+            e0.record(stream)
+            e0.synchronize()
+            times.append(s0.elapsed_time(e0))
+            stats = f.stats()
+            blob = f.serialize()
+            f.close()
+        e2e = []
+        for _ in range(e2e_steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            f = rsb.GPURecSplit(host_keys, bucket_size=b, leaf_size=leaf, key_type=kind, engine=engine)
+            blob2 = f.serialize()
             e2e.append(time.perf_counter() - t0)
-        bits = f.get_bits()
-        f.close()
+            bits = f.get_bits()
+            f.close()
     parity = None
     if os.path.exists(GOLDEN):
         g = json.load(open(GOLDEN)).get(golden)
         if g is not None:
-            parity = {"sha256_equals_oracle": hashlib.sha256(blob).hexdigest() == g["sha256"], "golden": golden}
+            parity = {"sha256_equals_reference": hashlib.sha256(blob).hexdigest() == g["ref_sha256"]
+                      and hashlib.sha256(blob2).hexdigest() == g["ref_sha256"], "golden": golden}
     ms = statistics.median(times)
     ms_search = stats["ms_search"]
-    line = {
-        "metric": f"build ns/key ({args.mode}: {kind} keys, l={leaf}, b={b}, n={n})", "value": ms * 1e6 / n,
-        "unit": "ns/key", "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+    out = {
+        "metric": f"build ns/key ({name}: {kind} keys, l={leaf}, b={b}, n={n})", "value": ms * 1e6 / n,
+        "unit": "ns/key", "higher_is_better": False, "n_gpus": 1, "steps": steps,
+        "warmup": warmup, "warmup_kind": f"one-bucket builds (l={leaf})" if small_warmup else "same configuration",
         "ms_per_step": ms, "dtype": "u64", "data": "synthetic",
         "config": {"workload": f"{kind} keys n={n} (splitmix64 seed {seed}"
                                + (", printable 10-50 B strings" if kind == "strings" else "")
                                + f"), l={leaf}, b={b}, rotation", "l2": "flushed before every timed step"},
         "e2e": {"value": statistics.mean(e2e) * 1e9 / n, "unit": "ns/key", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": len(blob), "timing": "host wall clock around the public-API build"},
+                "d2h_bytes_per_step": len(blob2), "steps": e2e_steps,
+                "timing": "host wall clock around the public-API build and serialization"},
         "bits_per_key": bits / n, "parity": parity,
         "stage_ms": {"partition": stats["ms_partition"],
                      "search": {str(i): round(v, 3) for i, v in enumerate(ms_search) if v > 0},
                      "encode": stats["ms_encode"], "total": stats["ms_total"]},
         "stage_geval_s": {str(i): round(stats["evals_stage"][i] / (v * 1e-3) / 1e9, 1)
                           for i, v in enumerate(ms_search) if v > 0.05},
-        "gpu_launches": stats["kernel_launches"], "clocks": clocks.summary(),
+        "gpu_launches": stats["kernel_launches"] * steps, "clocks": clocks.summary(),
         "step_ms": [round(x, 3) for x in times],
     }
-    print(json.dumps(line), flush=True)
-    engine.close()
+    if own:
+        engine.close()
+    return out
 
 
-def run_batch(args) -> None:
+def measure_batch(nsets: int, engine=None) -> dict:
+    """Batched form: all sets in one pipeline vs back-to-back plain builds of the same sets on
+    the same engine; every set's function must equal its plain build."""
     import torch
     import gpurecsplit_b200 as rsb
 
     leaf, b = 12, 1000
     torch.cuda.set_device(0)
     stream = torch.cuda.current_stream()
-    engine = rsb.Engine(0, stream.cuda_stream)
-    keys, offsets = batch_workload(args.sets)
+    own = engine is None
+    if own:
+        engine = rsb.Engine(0, stream.cuda_stream)
+    keys, offsets = batch_workload(nsets)
     n = int(offsets[-1])
     keys_dev = torch.from_numpy(keys.view(np.int64)).to("cuda")
     torch.cuda.synchronize()
@@ -507,7 +603,7 @@ def run_batch(args) -> None:
 
     def plain_all():
         out = []
-        for i in range(args.sets):
+        for i in range(nsets):
             lo, hi = int(offsets[i]), int(offsets[i + 1])
             out.append(rsb.GPURecSplit.from_device(base + 8 * lo, hi - lo, b, leaf, key_type="u64", engine=engine,
                                                    device_only=False))
@@ -515,26 +611,31 @@ def run_batch(args) -> None:
 
     def timed(fn):
         torch.cuda.synchronize()
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record(stream)
+        s0, e0 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
         r = fn()
-        e.record(stream)
-        e.synchronize()
-        return r, s.elapsed_time(e)
+        e0.record(stream)
+        e0.synchronize()
+        return r, s0.elapsed_time(e0)
 
-    batched()  # warm-up (sizes the engine's scratch)
-    plain_all()
+    for f in batched()[0]:  # warm-up (sizes the engine's scratch)
+        f.close()
+    for f in plain_all():
+        f.close()
     with ClockSampler(0) as clocks:
         (funcs, st), t_batch = timed(batched)
         plain, t_plain = timed(plain_all)
     same = all(f.serialize() == p.serialize() for f, p in zip(funcs, plain))
-    line = {
+    for f in funcs + plain:
+        f.close()
+    del keys_dev
+    out = {
         "metric": "batched keys/s (log-uniform sets in [1e3,1e6], l=12, b=1000)", "value": n / (t_batch * 1e-3),
         "unit": "keys/s", "higher_is_better": True, "n_gpus": 1, "steps": 1, "warmup": 1,
         "ms_per_step": t_batch, "dtype": "u64", "data": "synthetic",
-        "config": {"workload": f"{args.sets} key sets, sizes round(exp(U[ln 1e3, ln 1e6])) (numpy seed 7), "
+        "config": {"workload": f"{nsets} key sets, sizes round(exp(U[ln 1e3, ln 1e6])) (numpy seed 7), "
                                f"set i = splitmix64(seed 1000+i) u64 keys, l={leaf}, b={b}, rotation",
-                   "sets": args.sets, "keys": n},
+                   "sets": nsets, "keys": n, "l2": f"inputs ({8 * n / 1e9:.1f} GB) larger than L2"},
         "plain_back_to_back": {"keys_per_s": n / (t_plain * 1e-3), "ms": t_plain},
         "speedup_vs_plain": t_plain / t_batch,
         "identical_to_plain": same,
@@ -545,8 +646,9 @@ def run_batch(args) -> None:
                           for i, v in enumerate(st["ms_search"]) if v > 0.05},
         "gpu_launches": st["kernel_launches"], "clocks": clocks.summary(),
     }
-    print(json.dumps(line), flush=True)
-    engine.close()
+    if own:
+        engine.close()
+    return out
 
 
 # ---------------------------------------------------------------------------------------
@@ -575,15 +677,18 @@ def serve_requests(nreq: int, pool_n: int, max_keys: int, seed: int = 11):
     return [(int(st), int(sz), SERVE_CLASSES[c]) for st, sz, c in zip(starts, sizes, cls)]
 
 
-def run_serve(args) -> None:
+def measure_serve(requests: int = 100, max_keys: int = 10_000_000, hbm_budget: int = 32 << 30, inflight: int = 2,
+                  load: float = 0.75) -> dict:
+    """Serving form: a saturated leg (every request queued at once: capacity), a Poisson leg at
+    `load` x capacity (p50/p99 latency), and each request alone (identity and sequential rate)."""
     import threading
 
     import torch
     import gpurecsplit_b200 as rsb
 
     torch.cuda.set_device(0)
-    data, offsets = string_pool(args.max_keys)
-    reqs = serve_requests(args.requests, args.max_keys, args.max_keys)
+    data, offsets = string_pool(max_keys)
+    reqs = serve_requests(requests, max_keys, max_keys)
     total_keys = sum(r[1] for r in reqs)
 
     def keys_of(r):
@@ -594,11 +699,11 @@ def run_serve(args) -> None:
         _, _, (leaf, b) = r
         return srv.submit_strings(keys_of(r), b, leaf)
 
-    srv = rsb.Server(hbm_budget=args.hbm_budget, inflight=args.inflight)
+    srv = rsb.Server(hbm_budget=hbm_budget, inflight=inflight)
     # Warm-up: 1M-key requests of every class on every worker size the engines' scratch.
-    wn = min(1_000_000, args.max_keys)
+    wn = min(1_000_000, max_keys)
     warm = [srv.submit_strings((data, offsets[:wn + 1]), b, leaf)
-            for _ in range(args.inflight) for leaf, b in SERVE_CLASSES]
+            for _ in range(inflight) for leaf, b in SERVE_CLASSES]
     for w in warm:
         srv.wait(w)
 
@@ -611,7 +716,7 @@ def run_serve(args) -> None:
         capacity = total_keys / t_sat
 
         # Poisson leg at `load` x capacity (arrival rate in requests/s).
-        rate = args.load * capacity / (total_keys / len(reqs))
+        rate = load * capacity / (total_keys / len(reqs))
         gaps = np.random.default_rng(5).exponential(1.0 / rate, len(reqs))
         ids = [None] * len(reqs)
         lag = []
@@ -655,18 +760,21 @@ def run_serve(args) -> None:
     per_class = {}
     for (st, n, (leaf, b)), l_ms in zip(reqs, lat):
         per_class.setdefault(f"l={leaf},b={b}", []).append(l_ms)
-    line = {
+    # every function handed out by the server is closed here; the alone builds were closed above
+    for f, _ in sat + poi:
+        f.close()
+    return {
         "metric": "serve keys/s (string requests, log-uniform [100,1e7] keys, mixed (l,b))",
         "value": capacity, "unit": "keys/s", "higher_is_better": True, "n_gpus": 1, "steps": 1, "warmup": 1,
         "ms_per_step": t_sat * 1e3, "dtype": "u64", "data": "synthetic",
-        "config": {"workload": f"{len(reqs)} requests; size round(exp(U[ln 100, ln {args.max_keys:.0e}])), "
-                               f"(l,b) uniform over {SERVE_CLASSES}, keys = slices of a pool of {args.max_keys} "
+        "config": {"workload": f"{len(reqs)} requests; size round(exp(U[ln 100, ln {max_keys:.0e}])), "
+                               f"(l,b) uniform over {SERVE_CLASSES}, keys = slices of a pool of {max_keys} "
                                "random 10-50 byte strings (numpy seed 2024), rotation",
-                   "requests": len(reqs), "keys": total_keys, "hbm_budget": args.hbm_budget,
-                   "inflight": args.inflight, "timing": "host wall clock (server steady clock for latency)"},
+                   "requests": len(reqs), "keys": total_keys, "hbm_budget": hbm_budget,
+                   "inflight": inflight, "timing": "host wall clock (server steady clock for latency)"},
         "saturated": {"keys_per_s": capacity, "s": t_sat,
                       "mean_batch_requests": float(np.mean([i["batch_requests"] for _, i in sat]))},
-        "poisson": {"load": args.load, "rate_req_per_s": rate, "keys_per_s": total_keys / t_poi, "s": t_poi,
+        "poisson": {"load": load, "rate_req_per_s": rate, "keys_per_s": total_keys / t_poi, "s": t_poi,
                     "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                     "queue_p50_ms": float(np.percentile(qwait, 50)), "queue_p99_ms": float(np.percentile(qwait, 99)),
                     "mean_batch_requests": float(batch_req.mean()), "max_submit_lag_ms": 1e3 * max(lag),
@@ -677,7 +785,6 @@ def run_serve(args) -> None:
         "identical_to_alone": bool(same),
         "clocks": clocks.summary(),
     }
-    print(json.dumps(line), flush=True)
 
 
 def main() -> None:
@@ -687,8 +794,7 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="rsb", choices=["rsb", "reference"])
     ap.add_argument("--n", type=int, default=N_KEYS)
-    ap.add_argument("--cpu-buckets", type=int, default=None, help="CPU baseline sample (default 192, 48 without AVX-512)")
-    ap.add_argument("--ref-buckets", type=int, default=None, help="reference-arm sample (default 96, 24 without AVX-512)")
+    ap.add_argument("--cpu-fraction", type=int, default=5, help="CPU baseline sample: 1/N of the workload's buckets")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", default="plain", choices=["plain", "batch", "serve", "c1", "c3"])
     ap.add_argument("--sets", type=int, default=1000)
@@ -697,16 +803,17 @@ def main() -> None:
     ap.add_argument("--hbm-budget", type=int, default=32 << 30)
     ap.add_argument("--inflight", type=int, default=2)
     ap.add_argument("--load", type=float, default=0.75)
+    ap.add_argument("--no-extras", action="store_true", help="omit the c1/c3/c4_batch/c5_serve keys of the default line")
     args = ap.parse_args()
     if args.mode == "batch":
-        run_batch(args)
+        print(json.dumps(measure_batch(args.sets)), flush=True)
         return
     if args.mode == "serve":
-        run_serve(args)
+        print(json.dumps(measure_serve(args.requests, args.max_keys, args.hbm_budget, args.inflight, args.load)),
+              flush=True)
         return
     if args.mode in CONFIGS:
-        args.warmup = max(args.warmup, 3)
-        run_config(args)
+        print(json.dumps(measure_config(args.mode, steps=args.steps, warmup=max(args.warmup, 3))), flush=True)
         return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

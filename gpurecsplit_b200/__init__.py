@@ -51,6 +51,7 @@ class Stats(ctypes.Structure):
         ("descriptor_bits", ctypes.c_uint64), ("ms_total", ctypes.c_double), ("ms_partition", ctypes.c_double),
         ("ms_search", ctypes.c_double * 21), ("ms_encode", ctypes.c_double),
         ("evals_stage", ctypes.c_uint64 * 21), ("kernel_launches", ctypes.c_uint64),
+        ("windows_stage", ctypes.c_uint64 * 21), ("window_candidates", ctypes.c_uint64 * 21),
     ]
 
     def as_dict(self) -> dict:
@@ -60,6 +61,7 @@ class Stats(ctypes.Structure):
             "descriptor_bits": self.descriptor_bits, "ms_total": self.ms_total,
             "ms_partition": self.ms_partition, "ms_search": list(self.ms_search), "ms_encode": self.ms_encode,
             "evals_stage": list(self.evals_stage), "kernel_launches": self.kernel_launches,
+            "windows_stage": list(self.windows_stage), "window_candidates": list(self.window_candidates),
         }
 
 

@@ -387,7 +387,11 @@ rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint
     S.keys = n;
     S.buckets = nb;
     S.evals_alg = h->ef.evals_alg;
-    for (int s = 0; s < kNumStages; ++s) S.evals_stage[s] = h->ef.evals_stage[s];
+    for (int s = 0; s < kNumStages; ++s) {
+        S.evals_stage[s] = h->ef.evals_stage[s];
+        S.windows_stage[s] = h->ef.windows_stage[s];
+        S.window_candidates[s] = window_candidates((int)leaf, s);
+    }
     S.kernel_launches = launches_so_far() - launches0;
     S.descriptor_bits = h->ef.total_bits;
     uint64_t tot = 0;
@@ -622,6 +626,8 @@ rsb_status build_batch_device(rsb_engine *e, const uint64_t *keys128, const uint
         S.evals_alg = totals.evals_alg;
         for (int s = 0; s < kNumStages; ++s) {
             S.evals_stage[s] = totals.evals_stage[s];
+            S.windows_stage[s] = totals.windows_stage[s];
+            S.window_candidates[s] = window_candidates((int)leaf, s);
             S.nodes_per_stage[s] = stage_counts[s];
             S.nodes += stage_counts[s];
         }

@@ -307,7 +307,7 @@ void launch_set_bucket_ids(const uint64_t *keys128, uint64_t n, const uint64_t *
                            uint32_t nsets, uint64_t nb_total, uint32_t *bucket_id, uint32_t *counts, cudaStream_t st) {
     cudaMemsetAsync(counts, 0, nb_total * sizeof(uint32_t), st);
     use_max_smem(k_set_bucket_ids);
-    k_set_bucket_ids<<<grid_for(n, kPartChunk, 148 * 6), kPartThreads, 0, st>>>((const ulonglong2 *)keys128, n, set_key,
+    k_set_bucket_ids<<<grid_for(n, kPartChunk, device_sm_count() * 6), kPartThreads, 0, st>>>((const ulonglong2 *)keys128, n, set_key,
                                                                                 set_bucket, nsets, bucket_id, counts);
     count_launches(1);
 }
@@ -318,7 +318,7 @@ void launch_set_scatter(const uint64_t *keys128, uint64_t n, const uint64_t *set
     cudaMemsetAsync(cursor, 0, nb_total * sizeof(uint32_t), st);
     const SetBuckets map{set_key, set_bucket, nsets, bucket_id};
     use_max_smem(k_chunk_scatter<SetBuckets>);
-    k_chunk_scatter<<<grid_for(n, kPartChunk, 148 * 6), kPartThreads, 0, st>>>((const ulonglong2 *)keys128, n, map, acc,
+    k_chunk_scatter<<<grid_for(n, kPartChunk, device_sm_count() * 6), kPartThreads, 0, st>>>((const ulonglong2 *)keys128, n, map, acc,
                                                                                cursor, sorted);
     count_launches(1);
 }
@@ -335,7 +335,7 @@ void launch_set_write_rice(const uint64_t *node_base, uint64_t nb_total, NodeArr
                            uint32_t nsets, const uint64_t *word_base, const uint64_t *set_bits, uint64_t *desc,
                            uint64_t cap_words, DevStatus *status, cudaStream_t st) {
     use_max_smem(k_set_write_rice);
-    k_set_write_rice<<<grid_for(nb_total * 32, 256, 148 * 8), 256, 0, st>>>(node_base, nb_total, nodes, tab, pos_acc,
+    k_set_write_rice<<<grid_for(nb_total * 32, 256, device_sm_count() * 8), 256, 0, st>>>(node_base, nb_total, nodes, tab, pos_acc,
                                                                           fixed_bits, set_bucket, nsets, word_base,
                                                                           set_bits, desc, cap_words, status);
     count_launches(1);

@@ -214,16 +214,18 @@ __global__ void k_ef_fill(const uint64_t *cum, const uint64_t *pos, uint64_t nb,
 // Algorithmic work of the searches: sum over nodes of (candidates up to the found seed) * m,
 // candidates being seeds (splits, brute-force leaves) or rotation bases (rotation leaves).
 __global__ void k_evals(const uint64_t *node_total, NodeArrays nodes, uint32_t leaf, uint32_t rotate, EfParams *ef) {
-    __shared__ unsigned long long s_acc[kNumStages];
-    for (int s = threadIdx.x; s < kNumStages; s += blockDim.x) s_acc[s] = 0;
+    __shared__ unsigned long long s_acc[kNumStages], s_win[kNumStages];
+    for (int s = threadIdx.x; s < kNumStages; s += blockDim.x) s_acc[s] = s_win[s] = 0;
     __syncthreads();
     const uint64_t n = *node_total;
     for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t x = nodes.seed[j];
         const uint32_t m = nodes.size[j];
+        const uint32_t stage = nodes.stage[j];
+        if (stage >= kStageUpper) atomicAdd(&s_win[stage], (unsigned long long)nodes.next_win[j]);
         if (x >= kSeedFailed) continue;
         const uint64_t trials = (rotate && m == leaf) ? x / leaf + 1 : x + 1;
-        atomicAdd(&s_acc[nodes.stage[j]], (unsigned long long)(trials * m));
+        atomicAdd(&s_acc[stage], (unsigned long long)(trials * m));
     }
     __syncthreads();
     for (int s = threadIdx.x; s < kNumStages; s += blockDim.x) {
@@ -231,6 +233,7 @@ __global__ void k_evals(const uint64_t *node_total, NodeArrays nodes, uint32_t l
             atomicAdd((unsigned long long *)&ef->evals_stage[s], s_acc[s]);
             atomicAdd((unsigned long long *)&ef->evals_alg, s_acc[s]);
         }
+        if (s_win[s]) atomicAdd((unsigned long long *)&ef->windows_stage[s], s_win[s]);
     }
 }
 
@@ -246,7 +249,7 @@ int grid_for(uint64_t n, int threads, int cap) {
 void launch_bucket_bits(const uint64_t *node_base, uint64_t nb, NodeArrays nodes, DevTables tab, uint32_t *bits,
                         uint32_t *fixed_bits, DevStatus *status, cudaStream_t st) {
     use_max_smem(k_bucket_bits);
-    k_bucket_bits<<<grid_for(nb * 32, 256, 148 * 8), 256, 0, st>>>(node_base, nb, nodes, tab, bits, fixed_bits, status);
+    k_bucket_bits<<<grid_for(nb * 32, 256, device_sm_count() * 8), 256, 0, st>>>(node_base, nb, nodes, tab, bits, fixed_bits, status);
     count_launches(1);
 }
 
@@ -254,7 +257,7 @@ void launch_write_rice(const uint64_t *node_base, uint64_t nb, NodeArrays nodes,
                        const uint32_t *fixed_bits, uint64_t *desc, uint64_t desc_cap_words, EfParams *ef,
                        DevStatus *status, cudaStream_t st) {
     use_max_smem(k_write_rice);
-    k_write_rice<<<grid_for(nb * 32, 256, 148 * 8), 256, 0, st>>>(node_base, nb, nodes, tab, pos_acc, fixed_bits, desc,
+    k_write_rice<<<grid_for(nb * 32, 256, device_sm_count() * 8), 256, 0, st>>>(node_base, nb, nodes, tab, pos_acc, fixed_bits, desc,
                                                                    desc_cap_words, ef, status);
     count_launches(1);
 }
@@ -265,18 +268,18 @@ void launch_ef_build(const uint64_t *cum, const uint64_t *pos, uint64_t nb, uint
     use_max_smem(k_ef_init);
     k_ef_init<<<1, 32, 0, st>>>(cum, pos, nb, ef);
     use_max_smem(k_ef_reduce);
-    k_ef_reduce<<<grid_for(nb, 256, 148 * 4), 256, 0, st>>>(cum, pos, nb, ef);
+    k_ef_reduce<<<grid_for(nb, 256, device_sm_count() * 4), 256, 0, st>>>(cum, pos, nb, ef);
     use_max_smem(k_ef_params);
     k_ef_params<<<1, 32, 0, st>>>(cum, pos, nb, ef, lower_cap, cum_cap, pos_cap, jump_cap, status);
     use_max_smem(k_ef_fill);
-    k_ef_fill<<<grid_for(nb + 1, 256, 148 * 8), 256, 0, st>>>(cum, pos, nb, ef, lower, upper_cum, upper_pos, jump, status);
+    k_ef_fill<<<grid_for(nb + 1, 256, device_sm_count() * 8), 256, 0, st>>>(cum, pos, nb, ef, lower, upper_cum, upper_pos, jump, status);
     count_launches(4);
 }
 
 void launch_evals(const uint64_t *node_total, NodeArrays nodes, uint32_t leaf, uint32_t rotate, EfParams *ef,
                   cudaStream_t st) {
     use_max_smem(k_evals);
-    k_evals<<<148 * 4, 256, 0, st>>>(node_total, nodes, leaf, rotate, ef);
+    k_evals<<<device_sm_count() * 4, 256, 0, st>>>(node_total, nodes, leaf, rotate, ef);
     count_launches(1);
 }
 

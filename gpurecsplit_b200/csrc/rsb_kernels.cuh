@@ -14,6 +14,9 @@ namespace rsb {
 // if neither kernel has the SMs configured with less shared memory than the other needs.
 // The kernels keep their working sets in shared memory and registers; L1 matters little.
 void prefer_shared_memory(const void *func);
+// Streaming multiprocessors of the current device (queried once per device); grid caps of
+// the non-persistent kernels are multiples of it.
+int device_sm_count();
 template <typename K>
 inline void use_max_smem(K kernel) {
     prefer_shared_memory((const void *)kernel);
@@ -79,6 +82,8 @@ void search_aggr(const SearchCtx &c, int stage, cudaStream_t st);
 void partition_aggr(const SearchCtx &c, int stage, cudaStream_t st);
 void search_leaves(const SearchCtx &c, int stage, cudaStream_t st);
 uint32_t search_slots_needed(int num_sms);
+// Candidates (seeds, or bases for rotation leaves) per window of a persistent search stage.
+uint32_t window_candidates(int leaf, int stage);
 
 // ---- encoding (rsb_encode.cu) ----
 struct EfParams {
@@ -90,6 +95,7 @@ struct EfParams {
     uint64_t desc_words;       // descriptor words incl. the sentinel
     uint64_t evals_alg;
     uint64_t evals_stage[kNumStages];
+    uint64_t windows_stage[kNumStages];  // candidate windows handed out by the persistent searches
 };
 
 // Kernels launched by this library (all threads), for the launch accounting of rsb_stats.

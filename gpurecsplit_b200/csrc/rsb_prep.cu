@@ -5,6 +5,7 @@
 //   string hashing            GPURecSplit.cuh:443-468, util/Hash128.h:32-36
 //   sort + partition          AbstractParallelRecSplit.hpp:339-359, src/Sorter.cpp:4-5
 //   grouping by bucket size   GPURecSplit.cuh:675-695
+#include <atomic>
 #include <mutex>
 #include <set>
 #include <utility>
@@ -354,14 +355,14 @@ int grid_for(uint64_t n, int threads, int cap) {
 
 void launch_hash_u64(const uint64_t *keys, uint64_t n, uint64_t *out128, cudaStream_t st) {
     use_max_smem(k_hash_u64);
-    k_hash_u64<<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(keys, n, (ulonglong2 *)out128);
+    k_hash_u64<<<grid_for(n, 256, device_sm_count() * 16), 256, 0, st>>>(keys, n, (ulonglong2 *)out128);
     count_launches(1);
 }
 
 void launch_hash_strings(const uint8_t *bytes, const uint64_t *offsets, uint64_t n, uint64_t base, uint64_t *out128,
                          cudaStream_t st) {
     use_max_smem(k_hash_strings);
-    k_hash_strings<<<grid_for(n, 128, 148 * 32), 128, 0, st>>>(bytes, offsets, n, base, (ulonglong2 *)out128);
+    k_hash_strings<<<grid_for(n, 128, device_sm_count() * 32), 128, 0, st>>>(bytes, offsets, n, base, (ulonglong2 *)out128);
     count_launches(1);
 }
 
@@ -369,18 +370,18 @@ void launch_bucket_count(const uint64_t *keys128, uint64_t n, uint64_t nb, uint3
     cudaMemsetAsync(counts, 0, nb * sizeof(uint32_t), st);
     if (nb <= kSmemHistMax) {
         use_max_smem(k_bucket_count_smem);
-        k_bucket_count_smem<<<grid_for(n, 512, 148 * 4), 512, nb * sizeof(uint32_t), st>>>((const ulonglong2 *)keys128, n,
+        k_bucket_count_smem<<<grid_for(n, 512, device_sm_count() * 4), 512, nb * sizeof(uint32_t), st>>>((const ulonglong2 *)keys128, n,
                                                                                             nb, counts);
     } else {
         use_max_smem(k_bucket_count_global);
-        k_bucket_count_global<<<grid_for(n, 256, 148 * 16), 256, 0, st>>>((const ulonglong2 *)keys128, n, nb, counts);
+        k_bucket_count_global<<<grid_for(n, 256, device_sm_count() * 16), 256, 0, st>>>((const ulonglong2 *)keys128, n, nb, counts);
     }
     count_launches(1);
 }
 
 void launch_bucket_check(const uint32_t *counts, uint64_t nb, DevStatus *status, cudaStream_t st) {
     use_max_smem(k_bucket_check);
-    k_bucket_check<<<grid_for(nb, 256, 148 * 8), 256, 0, st>>>(counts, nb, status);
+    k_bucket_check<<<grid_for(nb, 256, device_sm_count() * 8), 256, 0, st>>>(counts, nb, status);
     count_launches(1);
 }
 
@@ -388,7 +389,7 @@ void launch_bucket_scatter(const uint64_t *keys128, uint64_t n, uint64_t nb, con
                            uint64_t *sorted, cudaStream_t st) {
     cudaMemsetAsync(cursor, 0, nb * sizeof(uint32_t), st);
     use_max_smem(k_chunk_scatter<PlainBuckets>);
-    k_chunk_scatter<<<grid_for(n, kPartChunk, 148 * 6), kPartThreads, 0, st>>>((const ulonglong2 *)keys128, n,
+    k_chunk_scatter<<<grid_for(n, kPartChunk, device_sm_count() * 6), kPartThreads, 0, st>>>((const ulonglong2 *)keys128, n,
                                                                                PlainBuckets{nb}, acc, cursor, sorted);
     count_launches(1);
 }
@@ -396,27 +397,27 @@ void launch_bucket_scatter(const uint64_t *keys128, uint64_t n, uint64_t nb, con
 void launch_bucket_dupcheck(const uint64_t *sorted, const uint64_t *acc, uint64_t nb, DevStatus *status,
                             cudaStream_t st) {
     use_max_smem(k_bucket_dupcheck);
-    k_bucket_dupcheck<<<grid_for(nb, 1, 148 * 7), kSortThreads, 0, st>>>(sorted, acc, nb, status);
+    k_bucket_dupcheck<<<grid_for(nb, 1, device_sm_count() * 7), kSortThreads, 0, st>>>(sorted, acc, nb, status);
     count_launches(1);
 }
 
 void launch_bucket_nodes(const uint64_t *acc, uint64_t nb, DevTables tab, uint32_t *node_count, cudaStream_t st) {
     use_max_smem(k_bucket_nodes);
-    k_bucket_nodes<<<grid_for(nb, 256, 148 * 8), 256, 0, st>>>(acc, nb, tab, node_count);
+    k_bucket_nodes<<<grid_for(nb, 256, device_sm_count() * 8), 256, 0, st>>>(acc, nb, tab, node_count);
     count_launches(1);
 }
 
 void launch_tree_emit(const uint64_t *acc, uint64_t nb, const uint64_t *node_base, Shape sh, NodeArrays nodes,
                       cudaStream_t st) {
     use_max_smem(k_tree_emit);
-    k_tree_emit<<<grid_for(nb, 64, 148 * 16), 64, 0, st>>>(acc, nb, node_base, sh, nodes);
+    k_tree_emit<<<grid_for(nb, 64, device_sm_count() * 16), 64, 0, st>>>(acc, nb, node_base, sh, nodes);
     count_launches(1);
 }
 
 void launch_stage_lists(const uint8_t *stage, const uint64_t *total_nodes, uint32_t max_nodes, uint32_t *stage_info,
                         uint32_t *lists, cudaStream_t st) {
     cudaMemsetAsync(stage_info, 0, 3 * kNumStages * sizeof(uint32_t), st);
-    const int g = grid_for(max_nodes, 256, 148 * 8);
+    const int g = grid_for(max_nodes, 256, device_sm_count() * 8);
     use_max_smem(k_stage_hist);
     k_stage_hist<<<g, 256, 0, st>>>(stage, total_nodes, stage_info);
     use_max_smem(k_stage_bases);
@@ -426,6 +427,25 @@ void launch_stage_lists(const uint8_t *stage, const uint64_t *total_nodes, uint3
     count_launches(3);
 }
 
+
+int device_sm_count() {
+    constexpr int kMaxDev = 64;
+    static std::atomic<int> cache[kMaxDev];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) {
+        cudaGetLastError();
+        return 148;
+    }
+    int v = cache[dev].load(std::memory_order_relaxed);
+    if (v <= 0) {
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) {
+            cudaGetLastError();
+            return 148;  // B200's count; the attribute query does not fail on a working device
+        }
+        cache[dev].store(v, std::memory_order_relaxed);
+    }
+    return v;
+}
 
 void prefer_shared_memory(const void *func) {
     static std::mutex mu;

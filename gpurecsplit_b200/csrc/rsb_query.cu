@@ -16,7 +16,7 @@ __global__ void k_query(MphfView f, const ulonglong2 *__restrict__ keys, uint64_
 void launch_query_view(const MphfView &f, const uint64_t *keys128, uint64_t n, uint64_t *out, cudaStream_t st) {
     uint64_t g = (n + 255) / 256;
     if (g < 1) g = 1;
-    if (g > 148 * 16) g = 148 * 16;
+    if (g > device_sm_count() * 16) g = device_sm_count() * 16;
     use_max_smem(k_query);
     k_query<<<(int)g, 256, 0, st>>>(f, (const ulonglong2 *)keys128, n, out);
 }

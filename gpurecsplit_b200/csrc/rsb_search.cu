@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cstdio>
 
+#include "rsb_fp32.cuh"
 #include "rsb_kernels.cuh"
 
 namespace rsb {
@@ -53,37 +54,6 @@ __device__ __forceinline__ uint32_t shl_clamp(uint32_t a, uint32_t b) {
 
 // Low 16 bits of remix32(hi ^ lo) of a 64-bit candidate.
 __device__ __forceinline__ uint32_t hash16(uint64_t v) { return remix32(uint32_t(v >> 32) ^ uint32_t(v)) & 0xFFFFu; }
-
-// remix32 without its final xor-shift: hash16 = (z ^ z >> 16) & 0xFFFF = lo16(z) ^ hi16(z).
-__device__ __forceinline__ uint32_t remix32_core(uint32_t z) {
-    z ^= z >> 16;
-    z *= 0x85ebca6bu;
-    z ^= z >> 13;
-    return z * 0xc2b2ae35u;
-}
-
-// Starting value of a full node's part-index accumulator: the bits of the fp32 2^23.
-constexpr uint32_t kAccF0 = 0x4B000000u;
-
-// Adds the part index of one candidate, given z = remix32_core of its key + seed, to acc.
-// Full node (m = fan * SPLIT): the part index ((hash16 * m) >> 16) / SPLIT is
-// p = floor(hash16 * fan / 2^16). The bits kAccF0 | hash16 are the fp32 F = 2^23 + hash16, and
-// F * (fan / 2^16) = 128 fan + hash16 * fan / 2^16, so with acc an integer-valued fp32 in
-// [2^23, 2^24), where the spacing of fp32 values is 1, one fused multiply-add rounded toward
-// minus infinity gives exactly acc + 128 fan + p: acc counts 2^23 + 128 fan m + sum p after m
-// keys, which stays below 2^24 for every node (128 fan m < 2^23). The add runs on the FP32
-// pipes, beside the integer hash. Other nodes: with b = hash16 << 16, p = umulhi(b, mult) >> 28
-// for mult = ceil(m * 2^28 / SPLIT) (< 2^32 as m < 16 * SPLIT; exact for every 16-bit hash,
-// leaf size and node size, checked exhaustively).
-template <bool FULL>
-__device__ __forceinline__ void add_part(uint32_t z, uint32_t mult, float cf, uint32_t &acc) {
-    if (FULL) {
-        const uint32_t f = (z & 0xFFFFu) ^ __funnelshift_r(z, kAccF0 >> 16, 16);
-        acc = __float_as_uint(__fmaf_rd(__uint_as_float(f), cf, __uint_as_float(acc)));
-    } else {
-        acc += __umulhi((z << 16) ^ (z & 0xFFFF0000u), mult) >> 28;
-    }
-}
 
 // Keys of an aggregation node per phase-A pass: after each chunk the window is abandoned if
 // the node's best seed has dropped to its first candidate.
@@ -551,33 +521,6 @@ __device__ __forceinline__ uint32_t rotl_leaf(uint32_t v, uint32_t r) {
     return ((v << r) | (v >> (LEAF - r))) & full;
 }
 
-// Adds the bit of one key, given z = remix32_core of key + seed, to a left-mask sum. The
-// bit index p = remap16 = floor(hash16 * LEAF / 2^16) comes from one fp32 fused multiply-add
-// rounded toward minus infinity, as in add_part: F = 2^23 + hash16 (bits kAccF0 | hash16)
-// times LEAF / 2^16 plus 2^23 - 128 LEAF is exactly 2^23 + hash16 * LEAF / 2^16, which rounds
-// down to the integer-valued fp32 2^23 + p, whose bits are kAccF0 + p. Times 2^23 plus
-// 127 << 23 (mod 2^32) these bits become (127 + p) << 23, the fp32 2^p, which is added to the
-// fp32 sum acc. Only the final integer add runs on the ALU pipe beside the hash.
-template <int LEAF>
-__device__ __forceinline__ void add_bit(uint32_t z, uint32_t &acc) {
-    constexpr float kScale = (float)LEAF * 0x1p-16f, kBias = 0x1p23f - 128.0f * LEAF;
-    const uint32_t f = (z & 0xFFFFu) ^ __funnelshift_r(z, kAccF0 >> 16, 16);
-    const uint32_t t = __float_as_uint(__fmaf_rd(__uint_as_float(f), kScale, kBias));
-    acc = __float_as_uint(__fadd_rn(__uint_as_float(acc), __uint_as_float(t * (1u << 23) + (127u << 23))));
-}
-
-// The left mask of a sum formed by add_bit over nl keys, or ~0u when two keys share a bit.
-// Without a shared bit the terms are distinct powers of two below 2^LEAF <= 2^24, every
-// partial sum is an integer below 2^24 and exact in fp32, and the sum is the mask with nl
-// bits set. With one, either every partial sum stays below 2^24 (exact), and the carry leaves
-// fewer than nl bits set, or the sum reaches 2^24 or more, out of the mask's range.
-template <int LEAF>
-__device__ __forceinline__ uint32_t left_mask_of(uint32_t acc, uint32_t nl) {
-    static_assert(LEAF <= 24, "left-mask sums are exact below 2^24 only");
-    const uint32_t mk = __float2uint_rz(__uint_as_float(acc));
-    return (mk >> LEAF) == 0 && __popc(mk) == (int)nl ? mk : ~0u;
-}
-
 // Left-mask sums (add_bit) of the S bases x0 + lane + 32 s of a rotation-leaf window
 // (bu = SEED + x0*LEAF) over the nl < 32 left keys sk[0, nl), with moment_sums' per-key terms:
 // the window spans 32*S*LEAF seeds, each key's (K', L) goes to pk[0, nf) and the indexes of
@@ -922,6 +865,12 @@ void run_leaves(const SearchCtx &c, int stage, cudaStream_t st) {
 }  // namespace
 
 uint32_t search_slots_needed(int num_sms) { return (uint32_t)num_sms * 64u; }  // 64 resident warps per SM at most
+
+uint32_t window_candidates(int leaf, int stage) {
+    if (stage == kStageUpper || stage == kStageLower) return 32u * aggr_seeds_per_lane(leaf);
+    if (stage == kStageLeafRot || stage == kStageLeafBF) return 32u * kLeafSeedsPerLane;
+    return 0;
+}
 
 bool shape_matches_kernels(const Shape &s) { return s.lower == lower_of((int)s.leaf) && s.upper == upper_of((int)s.leaf); }
 

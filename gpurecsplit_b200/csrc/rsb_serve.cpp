@@ -76,6 +76,7 @@ struct Request {
     uint32_t batch_requests = 0;
     uint64_t batch_keys = 0;
     bool done = false;
+    bool waited = false;  // a caller is in rsb_server_wait for this request (at most one)
     rsb_status status = RSB_OK;
     rsb_mphf *result = nullptr;
 
@@ -356,9 +357,16 @@ rsb_status rsb_server_wait(rsb_server *S, uint64_t id, double timeout_s, rsb_mph
     auto it = S->requests.find(id);
     if (it == S->requests.end()) return RSB_ERR_BAD_ARG;
     Request *r = it->second;
+    // One waiter per request: the waiter that returns the result frees the request, so a
+    // second concurrent waiter would read freed memory. It is refused instead.
+    if (r->waited) return RSB_ERR_BAD_ARG;
+    r->waited = true;
     auto ready = [&] { return r->done; };
     if (timeout_s < 0) S->cv_done.wait(lock, ready);
-    else if (!S->cv_done.wait_for(lock, std::chrono::duration<double>(timeout_s), ready)) return RSB_ERR_TIMEOUT;
+    else if (!S->cv_done.wait_for(lock, std::chrono::duration<double>(timeout_s), ready)) {
+        r->waited = false;  // the request stays; it may be waited for again
+        return RSB_ERR_TIMEOUT;
+    }
     if (info) {
         info->submit_s = r->submit_s;
         info->admit_s = r->admit_s;
@@ -368,7 +376,7 @@ rsb_status rsb_server_wait(rsb_server *S, uint64_t id, double timeout_s, rsb_mph
     }
     const rsb_status st = r->status;
     *out = r->result;
-    S->requests.erase(it);
+    S->requests.erase(id);  // by key: submissions during the wait may have rehashed the map
     delete r;
     return st;
 }

@@ -9,14 +9,22 @@
 // is part of this library's image.
 //
 // The array is a file-scope __device__ variable, so every GPU that loads the library holds
-// it (kStaticScratchBytes, about 1.8 MiB) until the process exits. All calls on a device
-// share it and it keeps the last call's contents. The kernel reads only bytes the same call
-// has just copied in and every hash it writes is copied out, so nothing needs clearing
-// between calls. Two calls whose GPU work overlapped would race on the array; this entry
-// point prevents that by holding a process-wide lock until its stream has finished.
-// The first call on a device resolves the array's device address with
+// it (kStaticScratchBytes, about 1.8 MiB) until the process exits. It comes into existence
+// when the CUDA runtime loads this library's device code on a device: at the first call
+// under lazy module loading (the CUDA 12 default), or when the context is created under
+// CUDA_MODULE_LOADING=EAGER. A caller whose memory pool will claim all device memory should
+// therefore make one small call on each device before the pool takes the memory. All calls
+// on a device share the array and it keeps the last call's contents. The kernel reads only
+// bytes the same call has just copied in and every hash it writes is copied out, so nothing
+// needs clearing between calls. Two calls whose GPU work overlapped would race on the array;
+// this entry point prevents that by holding a process-wide lock until its stream has
+// finished. The first call on a device resolves the array's device address with
 // cudaGetSymbolAddress (with that device current); make that first call before any stream
-// capture begins. Limits: 32,768 keys and 1 MiB of key bytes per call.
+// capture begins. Every call copies through pageable host memory and waits for its stream,
+// so a call whose stream is capturing is refused (RSB_ERR_BAD_ARG) before any work, which
+// leaves the caller's capture intact. Limits: 32,768 keys and 1 MiB of key bytes per call,
+// counted from offsets[0] (key i is bytes[offsets[i] .. offsets[i+1]), and only
+// bytes[offsets[0] .. offsets[n]) is copied).
 #include <cstring>
 #include <mutex>
 
@@ -62,15 +70,26 @@ extern "C" rsb_status rsb_hash_strings_static(const uint8_t *bytes, const uint64
     if (n > kStaticMaxKeys) return RSB_ERR_BAD_ARG;  // more keys than the static array holds
     for (uint64_t i = 0; i < n; ++i)
         if (offsets[i + 1] < offsets[i]) return RSB_ERR_BAD_ARG;
-    if (offsets[n] > kStaticMaxBytes || offsets[0] > offsets[n]) return RSB_ERR_BAD_ARG;
-    if (offsets[n] && !bytes) return RSB_ERR_BAD_ARG;
+    const uint64_t first = offsets[0];
+    const uint64_t nbytes = offsets[n] - first;  // offsets are non-decreasing (checked above)
+    if (nbytes > kStaticMaxBytes) return RSB_ERR_BAD_ARG;
+    if (nbytes && !bytes) return RSB_ERR_BAD_ARG;
     if (n == 0) return RSB_OK;
+    // An error left pending on this thread by earlier, unrelated CUDA work is not ours to
+    // report or clear: refuse the call and leave it in place for its owner.
+    if (cudaPeekAtLastError() != cudaSuccess) return RSB_ERR_CUDA;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
         cudaGetLastError();
         return RSB_ERR_NO_DEVICE;
     }
     cudaStream_t st = (cudaStream_t)stream;
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &capture) != cudaSuccess) {
+        cudaGetLastError();
+        return RSB_ERR_CUDA;
+    }
+    if (capture != cudaStreamCaptureStatusNone) return RSB_ERR_BAD_ARG;
     std::lock_guard<std::mutex> lock(g_static_mu);
     uint8_t *base = nullptr;
     if (static_scratch(dev, &base) != cudaSuccess) {
@@ -80,12 +99,14 @@ extern "C" rsb_status rsb_hash_strings_static(const uint8_t *bytes, const uint64
     uint8_t *d_bytes = base + kOffBytes;
     uint64_t *d_offsets = (uint64_t *)(base + kOffOffsets);
     uint64_t *d_hashes = (uint64_t *)(base + kOffHashes);
-    const uint64_t nbytes = offsets[n];
     bool ok = true;
-    if (nbytes) ok &= cudaMemcpyAsync(d_bytes, bytes, nbytes, cudaMemcpyHostToDevice, st) == cudaSuccess;
+    if (nbytes) ok &= cudaMemcpyAsync(d_bytes, bytes + first, nbytes, cudaMemcpyHostToDevice, st) == cudaSuccess;
     ok &= cudaMemcpyAsync(d_offsets, offsets, (n + 1) * 8, cudaMemcpyHostToDevice, st) == cudaSuccess;
-    if (ok) launch_hash_strings(d_bytes, d_offsets, n, 0, d_hashes, st);
-    ok &= cudaGetLastError() == cudaSuccess;
+    if (ok) {
+        // the kernel reads key i at d_bytes[offsets[i] - first]
+        launch_hash_strings(d_bytes, d_offsets, n, first, d_hashes, st);
+        ok &= cudaGetLastError() == cudaSuccess;  // nothing was pending at entry: this launch's own status
+    }
     if (ok) ok &= cudaMemcpyAsync(out, d_hashes, n * 16, cudaMemcpyDeviceToHost, st) == cudaSuccess;
     ok &= cudaStreamSynchronize(st) == cudaSuccess;
     if (!ok) {

@@ -69,6 +69,8 @@ typedef struct rsb_stats {
     double ms_encode;              /* Rice + Elias-Fano */
     uint64_t evals_stage[21];      /* evals_alg split by search stage */
     uint64_t kernel_launches;      /* kernels this build launched */
+    uint64_t windows_stage[21];    /* candidate windows handed out per persistent search stage (17..20) */
+    uint64_t window_candidates[21];/* candidates (seeds; bases for rotation leaves) per window of that stage */
 } rsb_stats;
 
 /* ---- engine ------------------------------------------------------------------------ */
@@ -156,7 +158,10 @@ rsb_status rsb_server_submit_strings(rsb_server *server, const uint8_t *bytes, c
 rsb_status rsb_server_submit_hash128(rsb_server *server, const rsb_hash128 *keys, uint64_t n, uint64_t bucket_size,
                                      uint32_t leaf_size, uint32_t flags, uint64_t *id);
 /* Waits for request `id` (at most timeout_s seconds; < 0 waits without limit) and hands
- * over its function (the caller frees it with rsb_free). RSB_ERR_TIMEOUT if not done. */
+ * over its function (the caller frees it with rsb_free). RSB_ERR_TIMEOUT if not done (the
+ * request can be waited for again). One caller at a time may wait for a request: a second
+ * concurrent wait for the same id returns RSB_ERR_BAD_ARG, as does a wait for an id whose
+ * result was already handed over. */
 rsb_status rsb_server_wait(rsb_server *server, uint64_t id, double timeout_s, rsb_mphf **out, rsb_request_info *info);
 /* Stops accepting requests, finishes the queued ones and releases the engines. */
 rsb_status rsb_server_destroy(rsb_server *server);
@@ -195,15 +200,22 @@ rsb_status rsb_hash_u64(rsb_engine *engine, const uint64_t *keys, uint64_t n, ui
 /* rsb_hash_strings without any device allocation. No counterpart in the reference.
  * For callers that cannot allocate device memory (a plugin inside a host process that owns
  * all device memory through its own pool, or a serving thread that must not call cudaMalloc
- * because it can synchronise the device). Keys i is bytes[offsets[i] .. offsets[i+1]);
+ * because it can synchronise the device). Key i is bytes[offsets[i] .. offsets[i+1]); only
+ * bytes[offsets[0] .. offsets[n]) is read, so `offsets` may index into a larger buffer.
  * bytes, offsets and out are host memory; the work runs on the current device and on
  * `stream` (a cudaStream_t, NULL for the default stream) and is complete on return. The
  * results equal rsb_hash_strings'. Staging uses one fixed array of device memory inside the
  * library (about 1.8 MiB, held by every GPU that loads the library until exit), so at most
- * 32,768 keys and 1 MiB of key bytes per call: larger inputs return RSB_ERR_BAD_ARG. The
- * first call on a device resolves that array's address (cudaGetSymbolAddress); make it
- * before any stream capture. Calls share the array; a process-wide lock held until the
- * stream finishes keeps their GPU work from overlapping. */
+ * 32,768 keys and 1 MiB of key bytes (offsets[n] - offsets[0]) per call: larger inputs return
+ * RSB_ERR_BAD_ARG. The array is created when the library's device code is loaded on a
+ * device: at the first call under lazy module loading (the CUDA 12 default) or at context
+ * creation with CUDA_MODULE_LOADING=EAGER, so make one small call on each device before a
+ * memory pool claims all of its memory. The first call on a device also resolves the
+ * array's address (cudaGetSymbolAddress); make it before any stream capture. Each call copies
+ * through pageable host memory and waits for `stream`, so a stream that is capturing is
+ * refused with RSB_ERR_BAD_ARG before any work. A CUDA error already pending on the calling
+ * thread is left in place and the call returns RSB_ERR_CUDA. Calls share the array; a
+ * process-wide lock held until the stream finishes keeps their GPU work from overlapping. */
 rsb_status rsb_hash_strings_static(const uint8_t *bytes, const uint64_t *offsets, uint64_t n, rsb_hash128 *out,
                                    void *stream);
 

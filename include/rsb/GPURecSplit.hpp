@@ -147,10 +147,16 @@ class GPURecSplit {
         rsb_detail::check(rsb_query_hash128(h_, (const rsb_hash128 *)keys, n, out), "GPURecSplit::operator()");
     }
 
+    // The reference adds the size of its own object (AbstractParallelRecSplit.hpp:476-478):
+    // three size_t fields, the descriptor RiceBitVector (one sux Vector), and DoubleEF (four
+    // sux Vectors and ten 64-bit fields). sux's Vector is taken as three words (size,
+    // capacity, data pointer), so the count equals a reference build's on the same function.
+    static constexpr size_t kReferenceObjectBytes = 3 * 8 + 5 * (3 * 8) + 10 * 8;
+
     size_t getBits() {
         uint64_t bits = 0;
         rsb_detail::check(rsb_get_bits(h_, &bits), "GPURecSplit::getBits");
-        return (size_t)bits + 8 * sizeof(*this);
+        return (size_t)bits + 8 * kReferenceObjectBytes;
     }
 
     rsb_mphf *handle() const { return h_; }

@@ -26,9 +26,28 @@ _simd_lib = None
 STATUS = {0: "OK", 1: "BAD_ARG", 2: "DUPLICATE_KEY", 3: "BUCKET_TOO_LARGE", 4: "FORMAT"}
 
 
+# The reference's own SIMDRecSplit compiled from its sources (oracle/ref_harness.cpp with the
+# stand-ins in oracle/_ref_shim/); built only where the reference tree is present, used
+# prebuilt elsewhere.
+_REF_LIB_PATH = os.path.join(_HERE, "_ref", "libref_simdrs.so")
+_REF_CHECKED_LIB_PATH = os.path.join(_HERE, "_ref", "libref_simdrs_checked.so")
+_REF_FLAGS = ("avx2", "bmi2", "avx512f", "avx512cd", "avx512dq", "avx512bw", "avx512vl", "avx512_vpopcntdq")
+_ref_libs = {}
+
+
+def reference_tree():
+    """The GpuRecSplit source tree to compile oracle/_ref from, or None when absent."""
+    root = os.environ.get("RSB_REFERENCE_ROOT", "/root/reference")
+    return root if os.path.isfile(os.path.join(root, "include", "function", "SIMDRecSplit.hpp")) else None
+
+
 def build() -> str:
-    """Compiles the oracle library with the committed Makefile (no-op when up to date)."""
+    """Compiles the oracle libraries with the committed Makefile (no-op when up to date), and
+    the reference's own SIMDRecSplit into oracle/_ref/ when the reference tree is present."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    ref = reference_tree()
+    if ref is not None:
+        subprocess.run(["make", "-s", "-j2", "-C", _HERE, "ref", f"REF={ref}"], check=True)
     return _LIB_PATH
 
 
@@ -238,3 +257,114 @@ def search_aggr(seconds: np.ndarray, split: int, seed: int, simd: bool = False) 
 
 def remap16(x: int, n: int) -> int:
     return int(lib().orc_remap16(x, n))
+
+
+# ---------------------------------------------------------------------------------------
+# The reference's own SIMDRecSplit (oracle/_ref), compiled from its unmodified sources
+# ---------------------------------------------------------------------------------------
+def _cpu_flags() -> set:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    return set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    return set()
+
+
+def ref_available(checked: bool = False) -> bool:
+    """True when oracle/_ref holds the reference build and this CPU can run it."""
+    path = _REF_CHECKED_LIB_PATH if checked else _REF_LIB_PATH
+    return os.path.exists(path) and all(x in _cpu_flags() for x in _REF_FLAGS)
+
+
+def ref_lib(checked: bool = False):
+    """The reference's SIMDRecSplit build (release, or with assertions when `checked`)."""
+    if checked not in _ref_libs:
+        path = _REF_CHECKED_LIB_PATH if checked else _REF_LIB_PATH
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} is missing: build it with oracle.build() where the reference tree is present")
+        if not all(x in _cpu_flags() for x in _REF_FLAGS):
+            raise RuntimeError("this CPU lacks the AVX-512 features the reference build needs")
+        L = ctypes.CDLL(path)
+        L.ref_build.restype = ctypes.c_void_p
+        L.ref_build.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int,
+                                ctypes.c_int]
+        L.ref_encode.restype = ctypes.c_void_p
+        L.ref_encode.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32,
+                                 ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                 ctypes.POINTER(ctypes.c_int)]
+        L.ref_blob_len.restype = ctypes.c_uint64
+        L.ref_blob_len.argtypes = [ctypes.c_void_p]
+        L.ref_blob_copy.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.ref_blob_free.argtypes = [ctypes.c_void_p]
+        L.ref_query.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int, ctypes.c_void_p,
+                                ctypes.c_uint64, ctypes.c_void_p]
+        L.ref_get_bits.restype = ctypes.c_uint64
+        L.ref_get_bits.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int]
+        L.ref_object_size.restype = ctypes.c_uint64
+        L.ref_object_size.argtypes = [ctypes.c_uint32, ctypes.c_int]
+        _ref_libs[checked] = L
+    return _ref_libs[checked]
+
+
+def _ref_blob(L, h) -> np.ndarray:
+    n = L.ref_blob_len(h)
+    a = np.zeros(n, dtype=np.uint8)
+    if n:
+        L.ref_blob_copy(h, _ptr(a))
+    L.ref_blob_free(h)
+    return a
+
+
+def ref_build(keys128: np.ndarray, leaf: int, bucket_size: int, rotate: bool = True, threads: int = 0,
+              checked: bool = False) -> np.ndarray:
+    """Serialized function built by the reference's SIMDRecSplit<leaf, MALLOC, rotate> from
+    `keys128` (uint64 (n, 2): first, second) with `threads` threads."""
+    keys128 = np.ascontiguousarray(keys128, dtype=np.uint64).reshape(-1, 2)
+    threads = threads or os.cpu_count() or 1
+    L = ref_lib(checked)
+    h = L.ref_build(_ptr(keys128), keys128.shape[0], leaf, bucket_size, int(rotate), threads)
+    if not h:
+        raise RuntimeError("ref_build: bad arguments")
+    return _ref_blob(L, h)
+
+
+def ref_encode(bucket_keys: np.ndarray, bucket_size: int, leaf: int, seeds: np.ndarray, sizes: np.ndarray,
+               rotate: bool = True, checked: bool = False) -> np.ndarray:
+    """Serialized function made by the reference's RiceBitVector::Builder, DoubleEF and
+    operator<< from given DFS seeds and node sizes; `bucket_keys` holds the key count of
+    every bucket."""
+    bk = np.ascontiguousarray(bucket_keys, dtype=np.uint64)
+    sd = np.ascontiguousarray(seeds, dtype=np.uint64)
+    sz = np.ascontiguousarray(sizes, dtype=np.uint32)
+    L = ref_lib(checked)
+    err = ctypes.c_int(0)
+    h = L.ref_encode(_ptr(bk), bk.size, int(bk.sum()), bucket_size, leaf, int(rotate), _ptr(sd), _ptr(sz), sd.size,
+                     ctypes.byref(err))
+    if not h:
+        raise RuntimeError(f"ref_encode failed ({err.value})")
+    return _ref_blob(L, h)
+
+
+def ref_query(serialized: np.ndarray, leaf: int, keys128: np.ndarray, rotate: bool = True) -> np.ndarray:
+    """The reference's operator>> then operator()(hash128_t) for every key."""
+    serialized = np.ascontiguousarray(serialized, dtype=np.uint8)
+    keys128 = np.ascontiguousarray(keys128, dtype=np.uint64).reshape(-1, 2)
+    out = np.zeros(keys128.shape[0], dtype=np.uint64)
+    st = ref_lib().ref_query(_ptr(serialized), serialized.size, leaf, int(rotate), _ptr(keys128), keys128.shape[0],
+                             _ptr(out))
+    if st:
+        raise RuntimeError(f"ref_query: cannot read the function (status {st})")
+    return out
+
+
+def ref_get_bits(serialized: np.ndarray, leaf: int, rotate: bool = True) -> int:
+    serialized = np.ascontiguousarray(serialized, dtype=np.uint8)
+    return int(ref_lib().ref_get_bits(_ptr(serialized), serialized.size, leaf, int(rotate)))
+
+
+def ref_object_size(leaf: int, rotate: bool = True) -> int:
+    """sizeof(SIMDRecSplit<leaf, MALLOC, rotate>) in the reference build."""
+    return int(ref_lib().ref_object_size(leaf, int(rotate)))

@@ -55,6 +55,7 @@ int main(int argc, char **argv) {
     for (const auto &k : keys)
         if (back(k) != rs(k)) { std::puts("round trip differs"); return 1; }
     std::printf("bits/key %.4f\n", (double)rs.getBits() / keys.size());
+    std::printf("getBits %zu\n", rs.getBits());
 
     std::vector<std::string> words;
     for (int i = 0; i < 5000; ++i) words.push_back("key-" + std::to_string(i * 7919));

@@ -3,9 +3,9 @@
 Reads include/function/golombRiceMemo.hpp of ByteHamster/GpuRecSplit (23 rows of 3000
 uint32 for leaf sizes 2..24, AbstractParallelRecSplit.hpp:191-227 generates them) and
 records, per leaf size, the SHA-256 of the row as little-endian uint32 plus a few spot
-values. Run once where the reference is mounted:
+values. Run once where the reference source tree is present, giving its path:
 
-    python tests/golden/make_memo_digests.py /root/reference
+    python tests/golden/make_memo_digests.py <GpuRecSplit source tree>
 """
 import hashlib
 import json
@@ -38,4 +38,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_memo_digests.py <path of the GpuRecSplit source tree>")
+    main(sys.argv[1])

@@ -209,10 +209,17 @@ def _keys(oracle_mod, kind, seed, n):
     return ("strings", oracle_mod.keygen_strings(seed, n))
 
 
-@pytest.mark.parametrize("name", ["hash128_n100k_l12_b1000", "hash128_n50k_l8_b2000_bf", "u64_n100k_l16_b2000",
-                                  "hash128_n1M_l8_b100", "strings_n1M_l8_b100", "u64_n5M_l16_b2000",
-                                  "u64_n200k_l24_b2000"])
+GOLDEN_NAMES = ["hash128_n100k_l12_b1000", "hash128_n50k_l8_b2000_bf", "u64_n100k_l16_b2000", "hash128_n1M_l8_b100",
+                "strings_n1M_l8_b100", "u64_n5M_l16_b2000", "u64_n200k_l24_b2000", "u64_n5M_l18_b50",
+                "hash128_n1M_l8_b2", "hash128_n1M_l8_b5", "hash128_n1M_l5_b10", "hash128_n12345678_l8_b100",
+                "hash128_n10M_l4_b25", "hash128_n10M_l2_b2"]
+
+
+@pytest.mark.parametrize("name", GOLDEN_NAMES)
 def test_golden_digest(rsb, oracle_mod, engine, name):
+    """Full-size device builds against digests of the reference's own SIMDRecSplit builds;
+    the reference's operator>> and operator() (oracle/_ref) then read the device's function
+    as a bijection onto [0, n), key by key equal to this library's query."""
     g = _golden().get(name)
     if g is None:
         pytest.skip(f"no committed digest for {name}")
@@ -222,7 +229,14 @@ def test_golden_digest(rsb, oracle_mod, engine, name):
     blob = f.serialize()
     assert len(blob) == g["bytes"]
     assert hashlib.sha256(blob).hexdigest() == g["sha256"]
-    assert f.get_bits() == g["bits"]
+    assert hashlib.sha256(blob).hexdigest() == g.get("ref_sha256", g["sha256"])
+    assert f.get_bits(object_bytes=224 if "ref_sha256" in g else 0) == g["bits"]  # getBits() of the reference, object size included
+    if oracle_mod.ref_available():
+        k128 = keys if kind == "hash128" else (oracle_mod.hash_u64(keys) if kind == "u64"
+                                              else oracle_mod.hash_strings(*keys))
+        ref_vals = oracle_mod.ref_query(np.frombuffer(blob, dtype=np.uint8), g["leaf"], k128, g["rotate"])
+        assert np.array_equal(np.sort(ref_vals), np.arange(g["n"], dtype=np.uint64))
+        assert np.array_equal(ref_vals, f.query(k128))
 
 
 def test_string_keys_as_slice_of_larger_buffer(rsb, oracle_mod, engine):

@@ -28,3 +28,7 @@ def test_cpp_dropin(tmp_path, oracle_mod, rsb):
     keys = oracle_mod.keygen_hash128(0x5603141978c51071, 100000)
     ref = oracle_mod.build_mphf(keys, 8, 100)
     assert out.read_bytes() == ref.bytes.tobytes()
+    if oracle_mod.ref_available():
+        # getBits() as the reference's own SIMDRecSplit reports it for the same bytes
+        bits = int(next(l for l in r.stdout.splitlines() if l.startswith("getBits ")).split()[1])
+        assert bits == oracle_mod.ref_get_bits(ref.bytes, 8)

@@ -25,9 +25,8 @@ def test_cpp_dropin_compiles_and_links(tmp_path, rsb):
 
 
 def test_reference_arm_json_contract():
-    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
-                        "--warmup", "3", "--ref-buckets", "2"], capture_output=True, text=True, timeout=600,
-                       cwd=ROOT)
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "2",
+                        "--warmup", "3", "--n", "40000"], capture_output=True, text=True, timeout=600, cwd=ROOT)
     assert r.returncode == 0, r.stderr[-2000:]
     line = json.loads(r.stdout.strip().splitlines()[-1])
     for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
@@ -36,4 +35,29 @@ def test_reference_arm_json_contract():
     assert line["impl"] == "reference"
     assert line["unit"] == "ns/key" and line["higher_is_better"] is False
     assert line["value"] > 0 and line["e2e"]["value"] == line["value"]
-    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    assert line["cpu_baseline"]["kind"] in ("reference", "port") and line["cpu_baseline"]["cores"] >= 1
+    # the reference line's config is the GPU arm's config, so the two are the same workload
+    sys.path.insert(0, ROOT)
+    import bench
+    assert line["config"] == bench.workload_config(40000, 1)
+
+
+def test_cpu_bucket_ranges_rebuild_the_full_builds_searches(oracle_mod):
+    """bench.py times CPU builds on contiguous bucket ranges of the workload: each range,
+    built as its own function, must have the full build's bucket sizes and DFS seeds for those
+    buckets, so that ranges covering the workload do its search work exactly once."""
+    sys.path.insert(0, ROOT)
+    import bench
+    import numpy as np
+    n = 40_000
+    simd = oracle_mod.simd_supported()
+    work = bench.CpuWorkload(n)
+    full = oracle_mod.build_mphf(oracle_mod.hash_u64(bench.splitmix64_keys(bench.SEED, n)), bench.LEAF,
+                                 bench.BUCKET, simd=simd)
+    seeds = []
+    for lo, hi in work.ranges(3):
+        keys, b = work.range_keys(lo, hi)
+        part = oracle_mod.build_mphf(keys, bench.LEAF, b, simd=simd)
+        assert np.array_equal(np.diff(part.bucket_size_acc), np.diff(full.bucket_size_acc)[lo:hi])
+        seeds.append(part.seeds)
+    assert np.array_equal(np.concatenate(seeds), full.seeds)

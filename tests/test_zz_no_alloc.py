@@ -42,6 +42,55 @@ def test_static_hash_matches_allocating_entry_point_on_consecutive_calls():
         engine.close()
 
 
+def test_static_hash_of_a_slice_deep_inside_a_larger_buffer():
+    """offsets[0] > 0: only bytes[offsets[0] .. offsets[n]) is read and counted against the
+    1 MiB limit, as in rsb_hash_strings, so a window past the first MiB of a buffer works."""
+    import gpurecsplit_b200 as rsb
+    import torch
+
+    torch.cuda.set_device(0)
+    engine = rsb.Engine(0)
+    try:
+        data, offsets = _keys(4, 60000, 10, 50)  # about 1.8 MiB of key bytes in all
+        lo, hi = 40000, 45000
+        window = offsets[lo:hi + 1]
+        assert int(window[0]) > (1 << 20) and int(window[-1] - window[0]) < (1 << 20)
+        for _ in range(2):
+            got = rsb.hash_strings_static((data, window))
+            want = rsb.hash_strings((data, window), engine)
+            assert np.array_equal(got, want)
+    finally:
+        engine.close()
+
+
+def test_static_hash_refuses_a_capturing_stream():
+    """The call copies through pageable memory and waits for its stream, so while that
+    stream is being captured it returns BAD_ARG before doing any work."""
+    import gpurecsplit_b200 as rsb
+    import torch
+
+    torch.cuda.set_device(0)
+    keys = _keys(5, 100, 10, 20)
+    rsb.hash_strings_static(keys)  # first call on the device: resolves the array before capture
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    x = torch.zeros(16, device="cuda")
+    refused = None
+    with torch.cuda.graph(g, stream=s, capture_error_mode="relaxed"):
+        x.add_(1)  # the captured work of the graph; the hashing call adds none
+        try:
+            rsb.hash_strings_static(keys, stream=s.cuda_stream)
+        except rsb.RSBError as e:
+            refused = e.name
+    assert refused == "BAD_ARG"
+    g.replay()
+    torch.cuda.synchronize()
+    assert float(x.sum()) == 16.0
+    del g
+    torch.cuda.synchronize()
+    assert np.array_equal(rsb.hash_strings_static(keys), rsb.hash_strings(keys))
+
+
 def test_static_hash_rejects_oversized_input():
     import gpurecsplit_b200 as rsb
 
