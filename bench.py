@@ -413,13 +413,17 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
             "stage_geval_s": {str(i): round(st["evals_stage"][i] / (v * 1e-3) / 1e9, 1)
                               for i, v in enumerate(ms_search) if v > 0.05},
             "step_ms": [round(x, 3) for x in step_ms],
+            "schedule": schedule_of(engine, LEAF, n),
+            "windows_per_stage": {str(i): [st["windows_stage"][i], st["window_candidates"][i]]
+                                  for i in (17, 18, 19) if st["windows_stage"][i]},
         }
         if world == 1 and not args.no_extras:
             # The other configurations, each with its own clock record, parity and timing
             # (one GPU; at N > 1 the line carries the headline only).
             del keys_dev, flush
             torch.cuda.empty_cache()
-            line["c1"] = measure_config("c1", engine, steps=5, warmup=3, e2e_steps=2)
+            # 1.8 ms per C1 build: 300 timed steps keep the clock sampler (200 ms period) busy
+            line["c1"] = measure_config("c1", engine, steps=300, warmup=3, e2e_steps=2)
             line["c3"] = measure_config("c3", engine, steps=1, warmup=1, e2e_steps=1)
             line["c4_batch"] = measure_batch(args.sets, engine)
             line["c5_serve"] = measure_serve(args.requests, args.max_keys, args.hbm_budget, args.inflight, args.load)
@@ -474,6 +478,24 @@ CONFIGS = {
     "c1": ("strings", 42, 1_000_000, 8, 100, "strings_n1M_l8_b100"),
     "c3": ("u64", 43, 200_000, 24, 2000, "u64_n200k_l24_b2000"),
 }
+
+
+HAND_SET = {17: lambda leaf: 12 if leaf >= 12 else 8, 18: lambda leaf: 12 if leaf >= 12 else 8, 19: lambda leaf: 8}
+
+
+def schedule_of(engine, leaf: int, keys: int) -> dict:
+    """The engine's stage schedules for a build of `keys` keys: {stage: [per lane, occupancy %]}."""
+    cls = 1 if keys >= (1 << 20) else 0
+    return {str(st): list(engine.schedule(leaf, st, cls)) for st in (17, 18, 19)}
+
+
+def set_hand_schedule(engine, leaf: int, keys: int, on: bool) -> None:
+    """Overrides the tuned schedules with the fixed ones used before tuning (12 candidates per
+    lane for aggregation at l >= 12, 8 otherwise, 8 bases for rotation leaves, full
+    occupancy), or restores the tuned ones."""
+    cls = 1 if keys >= (1 << 20) else 0
+    for st, f in HAND_SET.items():
+        engine.set_schedule(leaf, st, cls, f(leaf) if on else 0, 100)
 
 
 def measure_config(name: str, engine=None, steps: int = 5, warmup: int = 3, e2e_steps: int = 2) -> dict:
@@ -546,12 +568,26 @@ def measure_config(name: str, engine=None, steps: int = 5, warmup: int = 3, e2e_
             e2e.append(time.perf_counter() - t0)
             bits = f.get_bits()
             f.close()
+    # the same timed steps with the fixed schedule used before tuning (same function)
+    set_hand_schedule(engine, leaf, n, True)
+    hand = []
+    for _ in range(steps):
+        flush.zero_()
+        s0, e0 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        f = device_build()
+        e0.record(stream)
+        e0.synchronize()
+        hand.append(s0.elapsed_time(e0))
+        same_hand = f.serialize() == blob
+        f.close()
+    set_hand_schedule(engine, leaf, n, False)
     parity = None
     if os.path.exists(GOLDEN):
         g = json.load(open(GOLDEN)).get(golden)
         if g is not None:
-            parity = {"sha256_equals_reference": hashlib.sha256(blob).hexdigest() == g["ref_sha256"]
-                      and hashlib.sha256(blob2).hexdigest() == g["ref_sha256"], "golden": golden}
+            parity = {"sha256_equals_reference": hashlib.sha256(blob).hexdigest() == g.get("ref_sha256")
+                      and hashlib.sha256(blob2).hexdigest() == g.get("ref_sha256"), "golden": golden}
     ms = statistics.median(times)
     ms_search = stats["ms_search"]
     out = {
@@ -573,6 +609,10 @@ def measure_config(name: str, engine=None, steps: int = 5, warmup: int = 3, e2e_
                           for i, v in enumerate(ms_search) if v > 0.05},
         "gpu_launches": stats["kernel_launches"] * steps, "clocks": clocks.summary(),
         "step_ms": [round(x, 3) for x in times],
+        "schedule": schedule_of(engine, leaf, n),
+        "untuned": {"ms_per_step": statistics.median(hand), "schedule": {str(s): [f(leaf), 100] for s, f in
+                                                                       HAND_SET.items()},
+                    "tuning_gain": statistics.median(hand) / ms, "identical": same_hand},
     }
     if own:
         engine.close()
@@ -625,8 +665,12 @@ def measure_batch(nsets: int, engine=None) -> dict:
     with ClockSampler(0) as clocks:
         (funcs, st), t_batch = timed(batched)
         plain, t_plain = timed(plain_all)
+        set_hand_schedule(engine, leaf, n, True)
+        (hand_funcs, _), t_hand = timed(batched)
+        set_hand_schedule(engine, leaf, n, False)
     same = all(f.serialize() == p.serialize() for f, p in zip(funcs, plain))
-    for f in funcs + plain:
+    same_hand = all(f.serialize() == h.serialize() for f, h in zip(funcs, hand_funcs))
+    for f in funcs + plain + hand_funcs:
         f.close()
     del keys_dev
     out = {
@@ -645,6 +689,9 @@ def measure_batch(nsets: int, engine=None) -> dict:
         "stage_geval_s": {str(i): round(st["evals_stage"][i] / (v * 1e-3) / 1e9, 1)
                           for i, v in enumerate(st["ms_search"]) if v > 0.05},
         "gpu_launches": st["kernel_launches"], "clocks": clocks.summary(),
+        "schedule": schedule_of(engine, leaf, n),
+        "untuned": {"ms_per_step": t_hand, "schedule": {str(s): [f(leaf), 100] for s, f in HAND_SET.items()},
+                    "tuning_gain": t_hand / t_batch, "identical": same_hand},
     }
     if own:
         engine.close()

@@ -27,6 +27,7 @@ RSB_ROTATE = 1
 RSB_KEYS_ON_DEVICE = 2
 RSB_DEVICE_ONLY = 4
 RSB_KEEP_SEEDS = 8
+RSB_VERIFY = 16
 
 STATUS_NAMES = {
     0: "OK", 1: "BAD_ARG", 2: "CUDA", 3: "OOM", 4: "DUPLICATE_KEY", 5: "SEARCH_BUDGET",
@@ -112,6 +113,11 @@ def lib():
             "rsb_build_batch_hash128": ([vp, vp, vp, u32, u64, u32, u32, vp, ctypes.POINTER(Stats)], i32),
             "rsb_build_batch_u64": ([vp, vp, vp, u32, u64, u32, u32, vp, ctypes.POINTER(Stats)], i32),
             "rsb_build_batch_strings": ([vp, vp, vp, vp, u32, u64, u32, u32, vp, ctypes.POINTER(Stats)], i32),
+            "rsb_build_part_hash128": ([vp, vp, u64, u64, u64, u64, u64, u32, u32, pp], i32),
+            "rsb_part_export": ([vp, vp, ctypes.POINTER(ctypes.c_size_t)], i32),
+            "rsb_engine_set_schedule": ([vp, u32, u32, u32, u32, u32], i32),
+            "rsb_engine_get_schedule": ([vp, u32, u32, u32, ctypes.POINTER(u32), ctypes.POINTER(u32)], i32),
+            "rsb_merge_parts": ([vp, vp, vp, u32, u32, u32, pp], i32),
             "rsb_server_create": ([i32, u64, u32, u64, pp], i32),
             "rsb_server_submit_strings": ([vp, vp, vp, u64, u64, u32, u32, ctypes.POINTER(u64)], i32),
             "rsb_server_submit_hash128": ([vp, vp, u64, u64, u32, u32, ctypes.POINTER(u64)], i32),
@@ -166,6 +172,21 @@ class Engine:
         """Runs the persistent search kernels at `percent` of full occupancy (rsb_engine_set_occupancy)."""
         _check(lib().rsb_engine_set_occupancy(self._h, percent), "rsb_engine_set_occupancy")
 
+    def set_schedule(self, leaf_size: int, stage: int, size_class: int, seeds_per_lane: int,
+                     occupancy_pct: int = 100) -> None:
+        """Schedule of one search stage (rsb_engine_set_schedule): 17/18 aggregation levels
+        (8, 12 or 16 seeds per lane), 19 rotation leaves (4, 8 or 12 bases per lane); size class
+        0 below 2^20 keys, 1 from 2^20. seeds_per_lane 0 restores the built-in schedule."""
+        _check(lib().rsb_engine_set_schedule(self._h, leaf_size, stage, size_class, seeds_per_lane, occupancy_pct),
+               "rsb_engine_set_schedule")
+
+    def schedule(self, leaf_size: int, stage: int, size_class: int):
+        """(seeds per lane, occupancy %) this engine uses for the stage (rsb_engine_get_schedule)."""
+        s, p = ctypes.c_uint32(), ctypes.c_uint32()
+        _check(lib().rsb_engine_get_schedule(self._h, leaf_size, stage, size_class, ctypes.byref(s), ctypes.byref(p)),
+               "rsb_engine_get_schedule")
+        return s.value, p.value
+
     def probe_eval_rate(self):
         """(evaluations per second, ms) of the synthetic remixAndRemap32 ceiling kernel."""
         r, ms = ctypes.c_double(), ctypes.c_double()
@@ -214,7 +235,7 @@ class GPURecSplit:
 
     def __init__(self, keys=None, bucket_size: int = 100, leaf_size: int = 8, rotate: bool = True,
                  engine: Optional[Engine] = None, key_type: Optional[str] = None, keep_seeds: bool = False,
-                 device_only: bool = False, _handle=None):
+                 device_only: bool = False, verify: bool = False, _handle=None):
         self.leaf_size = leaf_size
         self.bucket_size = bucket_size
         self.rotate = rotate
@@ -222,7 +243,8 @@ class GPURecSplit:
         if _handle is not None:
             return
         eng = engine or default_engine()
-        flags = (RSB_ROTATE if rotate else 0) | (RSB_KEEP_SEEDS if keep_seeds else 0) | (RSB_DEVICE_ONLY if device_only else 0)
+        flags = (RSB_ROTATE if rotate else 0) | (RSB_KEEP_SEEDS if keep_seeds else 0) | \
+            (RSB_DEVICE_ONLY if device_only else 0) | (RSB_VERIFY if verify else 0)
         h = ctypes.c_void_p()
         L = lib()
         if key_type is None:
@@ -343,6 +365,51 @@ class GPURecSplit:
             self.close()
         except Exception:
             pass
+
+
+def build_part(keys, nbuckets_total: int, bucket_lo: int, bucket_hi: int, bucket_size: int, leaf_size: int,
+               rotate: bool = True, engine: Optional[Engine] = None, n: Optional[int] = None) -> bytes:
+    """Builds the part of an ``nbuckets_total``-bucket function over buckets [bucket_lo,
+    bucket_hi) (rsb_build_part_hash128) and returns it exported (rsb_part_export).
+
+    ``keys`` are the (n, 2) uint64 hash128 keys of exactly those buckets, as a host array or
+    (with ``n``) a device pointer.
+    """
+    eng = engine or default_engine()
+    L = lib()
+    flags = RSB_ROTATE if rotate else 0
+    if isinstance(keys, np.ndarray):
+        k = np.ascontiguousarray(keys, dtype=np.uint64).reshape(-1, 2)
+        ptr, count = _ptr(k), k.shape[0]
+    else:
+        ptr, count = ctypes.c_void_p(int(keys)), int(n)
+        flags |= RSB_KEYS_ON_DEVICE
+    h = ctypes.c_void_p()
+    _check(L.rsb_build_part_hash128(eng.handle, ptr, count, nbuckets_total, bucket_lo, bucket_hi, bucket_size,
+                                    leaf_size, flags, ctypes.byref(h)), "build_part")
+    try:
+        size = ctypes.c_size_t(0)
+        _check(L.rsb_part_export(h, None, ctypes.byref(size)), "part_export")
+        buf = ctypes.create_string_buffer(size.value)
+        _check(L.rsb_part_export(h, buf, ctypes.byref(size)), "part_export")
+        return buf.raw[:size.value]
+    finally:
+        L.rsb_free(h)
+
+
+def merge_parts(parts, leaf_size: int, rotate: bool = True, engine: Optional[Engine] = None) -> "GPURecSplit":
+    """Merges exported parts that tile all buckets of one function, in bucket order
+    (rsb_merge_parts); the result equals the plain build of all their keys."""
+    eng = engine or default_engine()
+    parts = [bytes(p) for p in parts]
+    bufs = [ctypes.create_string_buffer(p, len(p)) for p in parts]
+    ptrs = (ctypes.c_void_p * len(parts))(*[ctypes.cast(b, ctypes.c_void_p) for b in bufs])
+    lens = (ctypes.c_size_t * len(parts))(*[len(p) for p in parts])
+    h = ctypes.c_void_p()
+    _check(lib().rsb_merge_parts(eng.handle, ptrs, lens, len(parts), leaf_size, RSB_ROTATE if rotate else 0,
+                                 ctypes.byref(h)), "merge_parts")
+    bucket_size = int(np.frombuffer(parts[0][64:72], dtype=np.uint64)[0])  # header word 8
+    return GPURecSplit(bucket_size=bucket_size, leaf_size=leaf_size, rotate=rotate, _handle=h)
 
 
 def build_batch(keys: np.ndarray, set_offsets, bucket_size: int, leaf_size: int, rotate: bool = True,
@@ -512,5 +579,5 @@ def hash_u64(keys: np.ndarray, engine: Optional[Engine] = None) -> np.ndarray:
     return out
 
 
-__all__ = ["GPURecSplit", "Engine", "Server", "build_batch", "RSBError", "lib", "build_library", "golomb_memo", "hash_strings", "hash_u64",
+__all__ = ["GPURecSplit", "Engine", "Server", "build_batch", "build_part", "merge_parts", "RSBError", "lib", "build_library", "golomb_memo", "hash_strings", "hash_u64",
            "default_engine", "LIB_PATH"]

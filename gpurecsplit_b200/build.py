@@ -36,7 +36,7 @@ def _sources():
 
 
 def _headers_mtime() -> float:
-    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h", ".inc"))]
     hs.append(os.path.join(INCLUDE, "rsb.h"))
     return max(os.path.getmtime(h) for h in hs)
 

@@ -82,12 +82,16 @@ struct rsb_engine {
     uint32_t budget_shift = 10;
     uint64_t budget_min = 1ull << 16;
     std::map<uint32_t, std::pair<uint32_t *, uint32_t *>> tables;  // (leaf, rotate) -> device memo, nodes
+    std::map<uint32_t, StageSchedule> schedules;  // (leaf, stage, size class) -> rsb_engine_set_schedule
+    int last_seeds_per_lane[kNumStages] = {};      // schedules of the last build's stages (rsb_stats)
     DBuf<uint64_t> keys128, raw_u64, offsets, sorted, acc, node_base, scan_tmp, pos_acc, seed;
     DBuf<uint32_t> counts, node_count, lists, stage_info, sched, slots, bits, fixed_bits, nstart, nwin;
     DBuf<uint16_t> nsize;
     DBuf<uint8_t> nstage, bytes;
     DBuf<DevStatus> status;
     DBuf<EfParams> efp;
+    DBuf<uint64_t> windows;  // candidate windows per search stage (rsb_stats)
+    DBuf<uint32_t> verify_seen;  // RSB_VERIFY: one bit per value of the function
     // batched construction
     DBuf<uint64_t> set_key, set_bucket, set_bits, word_base, ef_base, out_block;
     DBuf<uint32_t> set_nb, bucket_id, set_words, ef_words;
@@ -107,6 +111,10 @@ struct rsb_mphf {
     std::vector<uint64_t> desc, lower, upper_cum, upper_pos, jump;
     std::vector<uint64_t> seeds;
     std::vector<uint32_t> sizes;
+    // part builds (rsb_build_part_hash128): the range of the whole function's buckets and the
+    // per-bucket key and descriptor-bit offsets of the part
+    uint64_t part_lo = 0, part_hi = 0, part_nb_total = 0;
+    std::vector<uint64_t> bucket_acc, bucket_pos;
     rsb_stats stats{};
     const LeafTables *tab = nullptr;
 
@@ -198,21 +206,36 @@ rsb_status copy_to_host(rsb_mphf *h, cudaStream_t st) {
 
 // Every search stage in dependency order: fanout-2 depths, then each aggregation level
 // followed by its partition, then the leaves. Records the stage-boundary events.
-cudaError_t enqueue_searches(rsb_engine *e, const SearchCtx &sc, const LeafTables &lt, cudaStream_t st) {
+uint32_t schedule_key(uint32_t leaf, int stage, int size_class) { return leaf * 256u + (uint32_t)stage * 2u + size_class; }
+
+// The engine's schedule of one stage: a rsb_engine_set_schedule override or the built-in table.
+StageSchedule engine_schedule(const rsb_engine *e, uint32_t leaf, int stage, uint64_t keys) {
+    const int sc = schedule_size_class(keys);
+    auto it = e->schedules.find(schedule_key(leaf, stage, sc));
+    return it != e->schedules.end() ? it->second : default_schedule((int)leaf, stage, sc);
+}
+
+cudaError_t enqueue_searches(rsb_engine *e, const SearchCtx &sc, const LeafTables &lt, uint64_t keys, cudaStream_t st) {
     cudaError_t err;
+    const uint32_t leaf = sc.sh.leaf;
+    for (int s = 0; s < kNumStages; ++s) e->last_seeds_per_lane[s] = 0;
     for (uint32_t d = 0; d < lt.max_higher_depth && d < (uint32_t)kMaxHigherDepth; ++d) {
         search_higher(sc, (int)d, st);
         if ((err = cudaEventRecord(e->ev[2 + d], st)) != cudaSuccess) return err;
     }
     for (int stage : {kStageUpper, kStageLower}) {
         if ((err = cudaMemsetAsync(sc.slots, 0xFF, sc.nslots * sizeof(uint32_t), st)) != cudaSuccess) return err;
-        search_aggr(sc, stage, st);
+        const StageSchedule s = engine_schedule(e, leaf, stage, keys);
+        e->last_seeds_per_lane[stage] = s.seeds_per_lane;
+        search_aggr(sc, stage, s, st);
         partition_aggr(sc, stage, st);
         if ((err = cudaEventRecord(e->ev[2 + stage], st)) != cudaSuccess) return err;
     }
     for (int stage : {kStageLeafRot, kStageLeafBF}) {
         if ((err = cudaMemsetAsync(sc.slots, 0xFF, sc.nslots * sizeof(uint32_t), st)) != cudaSuccess) return err;
-        search_leaves(sc, stage, st);
+        const StageSchedule s = stage == kStageLeafRot ? engine_schedule(e, leaf, stage, keys) : StageSchedule{8, 100};
+        e->last_seeds_per_lane[stage] = s.seeds_per_lane;
+        search_leaves(sc, stage, s, st);
         if ((err = cudaEventRecord(e->ev[2 + stage], st)) != cudaSuccess) return err;
     }
     return cudaGetLastError();
@@ -232,12 +255,41 @@ void fill_stage_times(rsb_engine *e, const LeafTables &lt, rsb_stats &S) {
     S.ms_encode = elapsed(prev, e->ev[kNumEvents - 1]);
 }
 
+// View of a function's device copy for device queries.
+MphfView device_view(const rsb_mphf *h, const DevTables &tab) {
+    MphfView v{};
+    v.sh = h->tab->shape;
+    v.nbuckets = h->nbuckets;
+    v.desc = h->d_desc();
+    v.desc_words = h->ef.desc_words;
+    v.u_cum_keys = h->ef.u_cum_keys;
+    v.u_position = h->ef.u_position;
+    v.l_cum_keys = h->ef.l_cum_keys;
+    v.l_position = h->ef.l_position;
+    v.cum_keys_min_delta = h->ef.cum_keys_min_delta;
+    v.min_diff = h->ef.min_diff;
+    v.bits_per_key_fixed_point = h->ef.bits_per_key_fixed_point;
+    v.lower = h->d_lower();
+    v.upper_cum = h->d_cum();
+    v.upper_pos = h->d_pos();
+    v.jump = h->d_jump();
+    v.lower_words = h->ef.lower_words;
+    v.cum_words = h->ef.cum_words;
+    v.pos_words = h->ef.pos_words;
+    v.jump_words = h->ef.jump_words;
+    v.memo = tab.memo;
+    return v;
+}
+
 // The build proper. keys128 is device memory holding n (first, second) pairs.
 // `hash_keys` (optional) enqueues the key-hashing kernel that produces keys128; it runs
 // after the build's start event so that hashing is part of the measured build.
+// `nb_override` (part builds) sets the bucket count instead of ceil(n / bucket_size), and
+// `keep_buckets` keeps the per-bucket key and bit offsets on the host (rsb_part_export).
 rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint64_t bucket_size, uint32_t leaf,
                         uint32_t flags, rsb_mphf **out, bool keep_seeds,
-                        const std::function<void()> &hash_keys = std::function<void()>()) {
+                        const std::function<void()> &hash_keys = std::function<void()>(), uint64_t nb_override = 0,
+                        bool keep_buckets = false) {
     const bool rotate = (flags & RSB_ROTATE) != 0;
     const LeafTables &lt = leaf_tables(leaf, rotate);
     if (!shape_matches_kernels(lt.shape)) return RSB_ERR_INTERNAL;
@@ -245,7 +297,7 @@ rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint
     rsb_status rs = get_device_tables(e, lt, leaf, rotate, tab);
     if (rs != RSB_OK) return rs;
     cudaStream_t st = e->stream;
-    const uint64_t nb = std::max<uint64_t>(1, (n + bucket_size - 1) / bucket_size);
+    const uint64_t nb = nb_override ? nb_override : std::max<uint64_t>(1, (n + bucket_size - 1) / bucket_size);
     const uint64_t max_nodes = n + 1;
     const uint32_t nslots = search_slots_needed(e->num_sms);
 
@@ -274,6 +326,7 @@ rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint
     RSB_ENSURE(e->pos_acc, nb + 1);
     RSB_ENSURE(e->status, 1);
     RSB_ENSURE(e->efp, 1);
+    RSB_ENSURE(e->windows, kNumStages);
 
     auto *h = new (std::nothrow) rsb_mphf;
     if (!h) return RSB_ERR_OOM;
@@ -320,6 +373,7 @@ rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint
     if (hash_keys) hash_keys();
     RSB_CKH(cudaMemsetAsync(e->status.p, 0, sizeof(DevStatus), st));
     RSB_CKH(cudaMemsetAsync(e->efp.p, 0, sizeof(EfParams), st));
+    RSB_CKH(cudaMemsetAsync(e->windows.p, 0, kNumStages * sizeof(uint64_t), st));
     RSB_CKH(cudaMemsetAsync(e->sched.p, 0, 2 * kNumStages * sizeof(uint32_t), st));
 
     // ---- buckets ----
@@ -355,7 +409,7 @@ rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint
     sc.budget_min = e->budget_min;
     sc.num_sms = e->num_sms;
     sc.occupancy_pct = e->occupancy_pct;
-    RSB_CKH(enqueue_searches(e, sc, lt, st));
+    RSB_CKH(enqueue_searches(e, sc, lt, n, st));
 
     // ---- encoding ----
     launch_bucket_bits(e->node_base.p, nb, nodes, tab, e->bits.p, e->fixed_bits.p, e->status.p, st);
@@ -365,7 +419,7 @@ rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint
                       e->status.p, st);
     launch_ef_build(e->acc.p, e->pos_acc.p, nb, n, e->efp.p, h->d_lower(), h->lower_cap, h->d_cum(), h->cum_cap,
                     h->d_pos(), h->pos_cap, h->d_jump(), h->jump_cap, e->status.p, st);
-    launch_evals(node_total, nodes, leaf, rotate ? 1 : 0, e->efp.p, st);
+    launch_evals(node_total, nodes, leaf, rotate ? 1 : 0, e->efp.p, e->windows.p, st);
     RSB_CKH(cudaGetLastError());
     RSB_CKH(cudaEventRecord(e->ev[kNumEvents - 1], st));
     // Wait for the build before the pageable copies below: a device-to-host copy into pageable
@@ -377,7 +431,9 @@ rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint
     DevStatus dst{};
     uint32_t stage_counts[kNumStages];
     RSB_CKH(cudaMemcpyAsync(&dst, e->status.p, sizeof(dst), cudaMemcpyDeviceToHost, st));
+    uint64_t windows[kNumStages];
     RSB_CKH(cudaMemcpyAsync(&h->ef, e->efp.p, sizeof(EfParams), cudaMemcpyDeviceToHost, st));
+    RSB_CKH(cudaMemcpyAsync(windows, e->windows.p, sizeof(windows), cudaMemcpyDeviceToHost, st));
     RSB_CKH(cudaMemcpyAsync(stage_counts, e->stage_info.p, sizeof(stage_counts), cudaMemcpyDeviceToHost, st));
     RSB_CKH(cudaStreamSynchronize(st));
     if (dst.code != 0) return fail((rsb_status)dst.code);
@@ -389,8 +445,8 @@ rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint
     S.evals_alg = h->ef.evals_alg;
     for (int s = 0; s < kNumStages; ++s) {
         S.evals_stage[s] = h->ef.evals_stage[s];
-        S.windows_stage[s] = h->ef.windows_stage[s];
-        S.window_candidates[s] = window_candidates((int)leaf, s);
+        S.windows_stage[s] = windows[s];
+        S.window_candidates[s] = 32u * (uint32_t)e->last_seeds_per_lane[s];
     }
     S.kernel_launches = launches_so_far() - launches0;
     S.descriptor_bits = h->ef.total_bits;
@@ -411,6 +467,22 @@ rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint
             RSB_CKH(cudaMemcpy(sz.data(), e->nsize.p, tot * 2, cudaMemcpyDeviceToHost));
         }
         for (uint64_t i = 0; i < tot; ++i) h->sizes[i] = sz[i];
+    }
+    if (flags & RSB_VERIFY) {
+        RSB_CKH(ensure(e->verify_seen, (n + 31) / 32 + 1) == RSB_OK ? cudaSuccess : cudaErrorMemoryAllocation);
+        RSB_CKH(cudaMemsetAsync(e->status.p, 0, sizeof(DevStatus), st));
+        launch_verify(device_view(h, tab), keys128, n, e->acc.p, e->pos_acc.p, nb, e->verify_seen.p, e->status.p, st);
+        RSB_CKH(cudaGetLastError());
+        DevStatus vst{};
+        RSB_CKH(cudaMemcpyAsync(&vst, e->status.p, sizeof(vst), cudaMemcpyDeviceToHost, st));
+        RSB_CKH(cudaStreamSynchronize(st));
+        if (vst.code != 0) return fail(RSB_ERR_INTERNAL);
+    }
+    if (keep_buckets) {
+        h->bucket_acc.resize(nb + 1);
+        h->bucket_pos.resize(nb + 1);
+        RSB_CKH(cudaMemcpy(h->bucket_acc.data(), e->acc.p, (nb + 1) * 8, cudaMemcpyDeviceToHost));
+        RSB_CKH(cudaMemcpy(h->bucket_pos.data(), e->pos_acc.p, (nb + 1) * 8, cudaMemcpyDeviceToHost));
     }
     if (!(flags & RSB_DEVICE_ONLY)) {
         rsb_status s = copy_to_host(h, st);
@@ -449,6 +521,7 @@ rsb_status ensure_batch_buffers(rsb_engine *e, uint64_t n, uint64_t nb_total, ui
     RSB_ENSURE(e->pos_acc, nb_total + 1);
     RSB_ENSURE(e->status, 1);
     RSB_ENSURE(e->efp, 1);
+    RSB_ENSURE(e->windows, kNumStages);
     RSB_ENSURE(e->set_words, nsets);
     RSB_ENSURE(e->set_bits, nsets);
     RSB_ENSURE(e->word_base, nsets + 1);
@@ -506,6 +579,7 @@ rsb_status build_batch_device(rsb_engine *e, const uint64_t *keys128, const uint
     if (hash_keys) hash_keys();
     RSB_CK(cudaMemsetAsync(e->status.p, 0, sizeof(DevStatus), st));
     RSB_CK(cudaMemsetAsync(e->efp.p, 0, sizeof(EfParams), st));
+    RSB_CK(cudaMemsetAsync(e->windows.p, 0, kNumStages * sizeof(uint64_t), st));
     RSB_CK(cudaMemsetAsync(e->sched.p, 0, 2 * kNumStages * sizeof(uint32_t), st));
     RSB_CK(cudaMemcpyAsync(e->set_key.p, h_off, (nsets + 1) * 8, cudaMemcpyHostToDevice, st));
     // ---- buckets of all sets ----
@@ -543,7 +617,7 @@ rsb_status build_batch_device(rsb_engine *e, const uint64_t *keys128, const uint
     sc.budget_min = e->budget_min;
     sc.num_sms = e->num_sms;
     sc.occupancy_pct = e->occupancy_pct;
-    RSB_CK(enqueue_searches(e, sc, lt, st));
+    RSB_CK(enqueue_searches(e, sc, lt, n, st));
     // ---- per-set encoding ----
     launch_bucket_bits(e->node_base.p, nb_total, nodes, tab, e->bits.p, e->fixed_bits.p, e->status.p, st);
     exclusive_scan_u32(e->bits.p, e->pos_acc.p, nb_total, stmp, st);
@@ -559,7 +633,7 @@ rsb_status build_batch_device(rsb_engine *e, const uint64_t *keys128, const uint
     exclusive_scan_u32(jw, jb, nsets, stmp, st);
     launch_set_ef_fill(e->acc.p, e->pos_acc.p, e->set_bucket.p, nsets, e->set_ef.p, lb, cb, pb, jb, lower, ucum, upos,
                        jump, st);
-    launch_evals(node_total, nodes, leaf, rotate ? 1 : 0, e->efp.p, st);
+    launch_evals(node_total, nodes, leaf, rotate ? 1 : 0, e->efp.p, e->windows.p, st);
     RSB_CK(cudaGetLastError());
     RSB_CK(cudaEventRecord(e->ev[kNumEvents - 1], st));
     // Wait for the build before the pageable copies below: a device-to-host copy into pageable
@@ -574,7 +648,9 @@ rsb_status build_batch_device(rsb_engine *e, const uint64_t *keys128, const uint
     std::vector<EfParams> sef(nsets);
     std::vector<uint64_t> bases(4 * ((uint64_t)nsets + 1)), wbase(nsets + 1);
     RSB_CK(cudaMemcpyAsync(&dst, e->status.p, sizeof(dst), cudaMemcpyDeviceToHost, st));
+    uint64_t windows[kNumStages];
     RSB_CK(cudaMemcpyAsync(&totals, e->efp.p, sizeof(totals), cudaMemcpyDeviceToHost, st));
+    RSB_CK(cudaMemcpyAsync(windows, e->windows.p, sizeof(windows), cudaMemcpyDeviceToHost, st));
     RSB_CK(cudaMemcpyAsync(stage_counts, e->stage_info.p, sizeof(stage_counts), cudaMemcpyDeviceToHost, st));
     if (nsets) {
         RSB_CK(cudaMemcpyAsync(sef.data(), e->set_ef.p, nsets * sizeof(EfParams), cudaMemcpyDeviceToHost, st));
@@ -626,8 +702,8 @@ rsb_status build_batch_device(rsb_engine *e, const uint64_t *keys128, const uint
         S.evals_alg = totals.evals_alg;
         for (int s = 0; s < kNumStages; ++s) {
             S.evals_stage[s] = totals.evals_stage[s];
-            S.windows_stage[s] = totals.windows_stage[s];
-            S.window_candidates[s] = window_candidates((int)leaf, s);
+            S.windows_stage[s] = windows[s];
+            S.window_candidates[s] = 32u * (uint32_t)e->last_seeds_per_lane[s];
             S.nodes_per_stage[s] = stage_counts[s];
             S.nodes += stage_counts[s];
         }
@@ -741,7 +817,8 @@ rsb_status rsb_engine_destroy(rsb_engine *e) {
     release(e->node_base); release(e->scan_tmp); release(e->pos_acc); release(e->seed); release(e->counts);
     release(e->node_count); release(e->lists); release(e->stage_info); release(e->sched); release(e->slots);
     release(e->bits); release(e->fixed_bits); release(e->nstart); release(e->nwin); release(e->nsize);
-    release(e->nstage); release(e->bytes); release(e->status); release(e->efp);
+    release(e->nstage); release(e->bytes); release(e->status); release(e->efp); release(e->windows);
+    release(e->verify_seen);
     release(e->set_key); release(e->set_bucket); release(e->set_bits); release(e->word_base); release(e->ef_base);
     release(e->out_block); release(e->set_nb); release(e->bucket_id); release(e->set_words); release(e->ef_words);
     release(e->set_ef);
@@ -779,6 +856,34 @@ rsb_status rsb_engine_reserve(rsb_engine *e, uint64_t keys, uint64_t bucket_size
 rsb_status rsb_engine_set_occupancy(rsb_engine *e, uint32_t percent) {
     if (!e || percent == 0 || percent > 100) return RSB_ERR_BAD_ARG;
     e->occupancy_pct = (int)percent;
+    return RSB_OK;
+}
+
+rsb_status rsb_engine_set_schedule(rsb_engine *e, uint32_t leaf, uint32_t stage, uint32_t size_class,
+                                   uint32_t seeds_per_lane, uint32_t occupancy_pct) {
+    if (!e || leaf < 2 || leaf > (uint32_t)kMaxLeafSize || size_class > 1 ||
+        (stage != (uint32_t)kStageUpper && stage != (uint32_t)kStageLower && stage != (uint32_t)kStageLeafRot))
+        return RSB_ERR_BAD_ARG;
+    const uint32_t key = schedule_key(leaf, (int)stage, (int)size_class);
+    if (seeds_per_lane == 0) {
+        e->schedules.erase(key);
+        return RSB_OK;
+    }
+    const StageSchedule s{(int)seeds_per_lane, (int)occupancy_pct};
+    if (!schedule_valid((int)stage, s)) return RSB_ERR_BAD_ARG;
+    e->schedules[key] = s;
+    return RSB_OK;
+}
+
+rsb_status rsb_engine_get_schedule(rsb_engine *e, uint32_t leaf, uint32_t stage, uint32_t size_class,
+                                   uint32_t *seeds_per_lane, uint32_t *occupancy_pct) {
+    if (!e || !seeds_per_lane || !occupancy_pct || leaf < 2 || leaf > (uint32_t)kMaxLeafSize || size_class > 1 ||
+        (stage != (uint32_t)kStageUpper && stage != (uint32_t)kStageLower && stage != (uint32_t)kStageLeafRot))
+        return RSB_ERR_BAD_ARG;
+    auto it = e->schedules.find(schedule_key(leaf, (int)stage, (int)size_class));
+    const StageSchedule s = it != e->schedules.end() ? it->second : default_schedule((int)leaf, (int)stage, (int)size_class);
+    *seeds_per_lane = (uint32_t)s.seeds_per_lane;
+    *occupancy_pct = (uint32_t)s.occupancy_pct;
     return RSB_OK;
 }
 
@@ -936,6 +1041,227 @@ rsb_status rsb_build_batch_strings(rsb_engine *e, const uint8_t *bytes, const ui
                               [=] { launch_hash_strings(db, doff, n, sbase, k128, st); });
 }
 
+// ---- sharded construction: parts over bucket ranges, merged into one function ----------
+//
+// The reference's compute_thread splits the buckets into contiguous ranges, builds each
+// range's Rice stream separately and appends the streams in bucket order
+// (SIMDRecSplit.hpp:695-745); bucket ranges on several GPUs work the same way. A part is
+// built like a plain function whose buckets are the range's (k_part_first re-maps the first
+// halves; the second halves, which decide every seed, are unchanged); its export carries the
+// per-bucket key and bit offsets and its Rice bits; the merge concatenates the bits in bucket
+// order, appends the sentinel and builds the double Elias-Fano index over all buckets.
+
+static constexpr uint64_t kPartMagic = 0x3154524150425352ull;  // "RSBPART1"
+static rsb_status ensure_host(rsb_mphf *h);
+
+rsb_status rsb_build_part_hash128(rsb_engine *e, const rsb_hash128 *keys, uint64_t n, uint64_t nbuckets_total,
+                                  uint64_t bucket_lo, uint64_t bucket_hi, uint64_t bucket_size, uint32_t leaf,
+                                  uint32_t flags, rsb_mphf **out) {
+    rsb_status s = check_common(e, n, bucket_size, leaf, out);
+    if (s != RSB_OK) return s;
+    if ((n && !keys) || nbuckets_total == 0 || bucket_lo >= bucket_hi || bucket_hi > nbuckets_total ||
+        bucket_hi - bucket_lo >= (1ull << 32))
+        return RSB_ERR_BAD_ARG;
+    const uint64_t nbp = bucket_hi - bucket_lo;
+    s = ensure(e->keys128, 2 * n);
+    if (s != RSB_OK) return s;
+    s = ensure(e->status, 1);
+    if (s != RSB_OK) return s;
+    cudaStream_t st = e->stream;
+    if (n) {
+        RSB_CK(cudaMemcpyAsync(e->keys128.p, keys, n * 16,
+                               (flags & RSB_KEYS_ON_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+        RSB_CK(cudaMemsetAsync(e->status.p, 0, sizeof(DevStatus), st));
+        launch_part_first(e->keys128.p, n, nbuckets_total, bucket_lo, nbp, e->status.p, st);
+        RSB_CK(cudaGetLastError());
+        DevStatus dst{};
+        RSB_CK(cudaMemcpyAsync(&dst, e->status.p, sizeof(dst), cudaMemcpyDeviceToHost, st));
+        RSB_CK(cudaStreamSynchronize(st));
+        if (dst.code != 0) return (rsb_status)dst.code;  // a key outside the bucket range
+    }
+    rsb_mphf *h = nullptr;
+    s = build_device(e, e->keys128.p, n, bucket_size, leaf, flags & ~(uint32_t)RSB_DEVICE_ONLY, &h,
+                     (flags & kKeepSeeds) != 0, std::function<void()>(), nbp, true);
+    if (s != RSB_OK) return s;
+    h->part_lo = bucket_lo;
+    h->part_hi = bucket_hi;
+    h->part_nb_total = nbuckets_total;
+    *out = h;
+    return RSB_OK;
+}
+
+rsb_status rsb_part_export(rsb_mphf *h, uint8_t *buf, size_t *len) {
+    if (!h || !len || h->part_hi == 0 || h->bucket_acc.size() != h->nbuckets + 1) return RSB_ERR_BAD_ARG;
+    rsb_status s = ensure_host(h);
+    if (s != RSB_OK) return s;
+    const uint64_t nb = h->nbuckets, bits = h->bucket_pos[nb], words = (bits + 63) / 64;
+    const size_t need = 8 * (9 + 2 * (nb + 1) + words);
+    if (!buf) {
+        *len = need;
+        return RSB_OK;
+    }
+    if (*len < need || words > h->desc.size()) return RSB_ERR_BAD_ARG;
+    uint64_t *o = (uint64_t *)buf;  // caller's buffer: written with memcpy, no alignment needed
+    const uint64_t head[9] = {kPartMagic, h->leaf, h->rotate ? 1u : 0u, h->part_nb_total, h->part_lo, h->part_hi,
+                              h->keys_count, bits, h->bucket_size};
+    std::memcpy(o, head, sizeof(head));
+    std::memcpy(buf + 8 * 9, h->bucket_acc.data(), 8 * (nb + 1));
+    std::memcpy(buf + 8 * (9 + nb + 1), h->bucket_pos.data(), 8 * (nb + 1));
+    std::vector<uint64_t> d(h->desc.begin(), h->desc.begin() + words);
+    if (bits % 64) d[words - 1] &= (1ull << (bits % 64)) - 1;  // the part's sentinel is not part of it
+    std::memcpy(buf + 8 * (9 + 2 * (nb + 1)), d.data(), 8 * words);
+    *len = need;
+    return RSB_OK;
+}
+
+rsb_status rsb_merge_parts(rsb_engine *e, const uint8_t *const *parts, const size_t *lens, uint32_t nparts,
+                           uint32_t leaf_size, uint32_t flags, rsb_mphf **out) {
+    if (!e || !parts || !lens || !out || nparts == 0) return RSB_ERR_BAD_ARG;
+    struct Part {
+        uint64_t leaf, rotate, nb_total, lo, hi, keys, bits, bucket_size;
+        const uint8_t *acc, *pos, *desc;
+    };
+    std::vector<Part> ps(nparts);
+    for (uint32_t i = 0; i < nparts; ++i) {
+        if (!parts[i] || lens[i] < 8 * 9) return RSB_ERR_FORMAT;
+        uint64_t head[9];
+        std::memcpy(head, parts[i], sizeof(head));
+        Part &p = ps[i];
+        p = Part{head[1], head[2], head[3], head[4], head[5], head[6], head[7], head[8], nullptr, nullptr, nullptr};
+        if (head[0] != kPartMagic || p.lo >= p.hi || p.hi > p.nb_total || p.bits > 8 * (uint64_t)lens[i])
+            return RSB_ERR_FORMAT;
+        const uint64_t nb = p.hi - p.lo, words = (p.bits + 63) / 64;
+        if (nb > lens[i] / 16 || lens[i] != 8 * (9 + 2 * (nb + 1) + words)) return RSB_ERR_FORMAT;
+        p.acc = parts[i] + 8 * 9;
+        p.pos = p.acc + 8 * (nb + 1);
+        p.desc = p.pos + 8 * (nb + 1);
+        // offsets start at 0, never decrease and end at the part's key and bit counts
+        uint64_t a0 = 0, b0 = 0;
+        for (uint64_t j = 0; j <= nb; ++j) {
+            uint64_t a, b;
+            std::memcpy(&a, p.acc + 8 * j, 8);
+            std::memcpy(&b, p.pos + 8 * j, 8);
+            if ((j == 0 && (a | b)) || a < a0 || b < b0) return RSB_ERR_FORMAT;
+            a0 = a;
+            b0 = b;
+        }
+        if (a0 != p.keys || b0 != p.bits) return RSB_ERR_FORMAT;
+    }
+    // the parts must tile the buckets of one function in order
+    const Part &p0 = ps[0];
+    uint64_t n = 0, total_bits = 0;
+    for (uint32_t i = 0; i < nparts; ++i) {
+        const Part &p = ps[i];
+        if (p.leaf != p0.leaf || p.rotate != p0.rotate || p.nb_total != p0.nb_total || p.bucket_size != p0.bucket_size ||
+            p.lo != (i ? ps[i - 1].hi : 0))
+            return RSB_ERR_BAD_ARG;
+        n += p.keys;
+        total_bits += p.bits;
+    }
+    const uint64_t nb = p0.nb_total;
+    if (ps[nparts - 1].hi != nb || nb != std::max<uint64_t>(1, (n + p0.bucket_size - 1) / p0.bucket_size))
+        return RSB_ERR_BAD_ARG;
+    const uint32_t leaf = (uint32_t)p0.leaf;
+    const bool rotate = p0.rotate != 0;
+    if (leaf < 2 || leaf > (uint32_t)kMaxLeafSize || leaf != leaf_size || (((flags & RSB_ROTATE) != 0) != rotate))
+        return RSB_ERR_BAD_ARG;
+    RSB_CK(cudaSetDevice(e->device));
+
+    // global bucket offsets and the concatenated Rice stream, then the sentinel appendFixed(1, 1)
+    std::vector<uint64_t> acc(nb + 1), pos(nb + 1);
+    const uint64_t desc_words = (((total_bits + 1 + 7) / 8) + 7 + 7) / 8;  // RiceBitVector.hpp:77
+    std::vector<uint64_t> desc(desc_words + 1, 0);
+    uint64_t kbase = 0, bbase = 0;
+    for (const Part &p : ps) {
+        const uint64_t pnb = p.hi - p.lo;
+        for (uint64_t j = 0; j < pnb; ++j) {
+            uint64_t a, b;
+            std::memcpy(&a, p.acc + 8 * j, 8);
+            std::memcpy(&b, p.pos + 8 * j, 8);
+            acc[p.lo + j] = kbase + a;
+            pos[p.lo + j] = bbase + b;
+        }
+        const uint64_t words = (p.bits + 63) / 64, sh = bbase % 64, w0 = bbase / 64;
+        for (uint64_t k = 0; k < words; ++k) {
+            uint64_t v;
+            std::memcpy(&v, p.desc + 8 * k, 8);
+            desc[w0 + k] |= v << sh;
+            if (sh && w0 + k + 1 < desc.size()) desc[w0 + k + 1] |= v >> (64 - sh);
+        }
+        kbase += p.keys;
+        bbase += p.bits;
+    }
+    acc[nb] = kbase;
+    pos[nb] = bbase;
+    desc[total_bits / 64] |= 1ull << (total_bits % 64);
+    desc.resize(desc_words);
+
+    const LeafTables &lt = leaf_tables(leaf, rotate);
+    cudaStream_t st = e->stream;
+    rsb_status s = ensure(e->acc, nb + 1);
+    if (s == RSB_OK) s = ensure(e->pos_acc, nb + 1);
+    if (s == RSB_OK) s = ensure(e->status, 1);
+    if (s == RSB_OK) s = ensure(e->efp, 1);
+    if (s != RSB_OK) return s;
+    auto *h = new (std::nothrow) rsb_mphf;
+    if (!h) return RSB_ERR_OOM;
+    h->leaf = leaf;
+    h->rotate = rotate;
+    h->bucket_size = p0.bucket_size;
+    h->keys_count = n;
+    h->nbuckets = nb;
+    h->tab = &lt;
+    h->device = e->device;
+    h->desc_cap = desc_words;
+    h->lower_cap = ((nb + 1) * 56 + 63) / 64 + 2;
+    h->cum_cap = (3 * (nb + 1) + 63) / 64 + 2;
+    h->pos_cap = h->cum_cap;
+    h->jump_cap = jump_words_for(nb) + 2;
+    const uint64_t block_words = h->desc_cap + h->lower_cap + h->cum_cap + h->pos_cap + h->jump_cap;
+    auto fail = [&](rsb_status r) {
+        if (h->d_block) cudaFree(h->d_block);
+        delete h;
+        return r;
+    };
+    if (cudaMalloc((void **)&h->d_block, block_words * 8) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(RSB_ERR_OOM);
+    }
+#define RSB_CKM(call)                  \
+    do {                               \
+        cudaError_t e_ = (call);       \
+        if (e_ != cudaSuccess) {       \
+            g_last_cuda = e_;          \
+            cudaStreamSynchronize(st); \
+            return fail(RSB_ERR_CUDA); \
+        }                              \
+    } while (0)
+    RSB_CKM(cudaMemsetAsync(h->d_block, 0, block_words * 8, st));
+    RSB_CKM(cudaMemcpyAsync(h->d_desc(), desc.data(), desc_words * 8, cudaMemcpyHostToDevice, st));
+    RSB_CKM(cudaMemcpyAsync(e->acc.p, acc.data(), (nb + 1) * 8, cudaMemcpyHostToDevice, st));
+    RSB_CKM(cudaMemcpyAsync(e->pos_acc.p, pos.data(), (nb + 1) * 8, cudaMemcpyHostToDevice, st));
+    RSB_CKM(cudaMemsetAsync(e->status.p, 0, sizeof(DevStatus), st));
+    RSB_CKM(cudaMemsetAsync(e->efp.p, 0, sizeof(EfParams), st));
+    launch_ef_build(e->acc.p, e->pos_acc.p, nb, n, e->efp.p, h->d_lower(), h->lower_cap, h->d_cum(), h->cum_cap,
+                    h->d_pos(), h->pos_cap, h->d_jump(), h->jump_cap, e->status.p, st);
+    RSB_CKM(cudaGetLastError());
+    DevStatus dst{};
+    RSB_CKM(cudaMemcpyAsync(&dst, e->status.p, sizeof(dst), cudaMemcpyDeviceToHost, st));
+    RSB_CKM(cudaMemcpyAsync(&h->ef, e->efp.p, sizeof(EfParams), cudaMemcpyDeviceToHost, st));
+    RSB_CKM(cudaStreamSynchronize(st));
+#undef RSB_CKM
+    if (dst.code != 0) return fail((rsb_status)dst.code);
+    h->ef.total_bits = total_bits;
+    h->ef.desc_words = desc_words;
+    h->stats.keys = n;
+    h->stats.buckets = nb;
+    h->stats.descriptor_bits = total_bits;
+    s = copy_to_host(h, st);
+    if (s != RSB_OK) return fail(s);
+    *out = h;
+    return RSB_OK;
+}
+
 rsb_status rsb_hash_strings(rsb_engine *e, const uint8_t *bytes, const uint64_t *offsets, uint64_t n, uint32_t flags,
                             rsb_hash128 *out) {
     if (!e || !offsets || !out) return RSB_ERR_BAD_ARG;
@@ -1032,27 +1358,7 @@ rsb_status rsb_query_device(rsb_engine *e, rsb_mphf *h, const rsb_hash128 *keys,
     DevTables tab;
     rsb_status s = get_device_tables(e, *h->tab, h->leaf, h->rotate, tab);
     if (s != RSB_OK) return s;
-    MphfView v{};
-    v.sh = h->tab->shape;
-    v.nbuckets = h->nbuckets;
-    v.desc = h->d_desc();
-    v.desc_words = h->ef.desc_words;
-    v.u_cum_keys = h->ef.u_cum_keys;
-    v.u_position = h->ef.u_position;
-    v.l_cum_keys = h->ef.l_cum_keys;
-    v.l_position = h->ef.l_position;
-    v.cum_keys_min_delta = h->ef.cum_keys_min_delta;
-    v.min_diff = h->ef.min_diff;
-    v.bits_per_key_fixed_point = h->ef.bits_per_key_fixed_point;
-    v.lower = h->d_lower();
-    v.upper_cum = h->d_cum();
-    v.upper_pos = h->d_pos();
-    v.jump = h->d_jump();
-    v.lower_words = h->ef.lower_words;
-    v.cum_words = h->ef.cum_words;
-    v.pos_words = h->ef.pos_words;
-    v.jump_words = h->ef.jump_words;
-    v.memo = tab.memo;
+    const MphfView v = device_view(h, tab);
     launch_query_view(v, (const uint64_t *)keys, n, out, e->stream);
     RSB_CK(cudaGetLastError());
     RSB_CK(cudaStreamSynchronize(e->stream));

@@ -213,7 +213,8 @@ __global__ void k_ef_fill(const uint64_t *cum, const uint64_t *pos, uint64_t nb,
 
 // Algorithmic work of the searches: sum over nodes of (candidates up to the found seed) * m,
 // candidates being seeds (splits, brute-force leaves) or rotation bases (rotation leaves).
-__global__ void k_evals(const uint64_t *node_total, NodeArrays nodes, uint32_t leaf, uint32_t rotate, EfParams *ef) {
+__global__ void k_evals(const uint64_t *node_total, NodeArrays nodes, uint32_t leaf, uint32_t rotate, EfParams *ef,
+                        uint64_t *windows) {
     __shared__ unsigned long long s_acc[kNumStages], s_win[kNumStages];
     for (int s = threadIdx.x; s < kNumStages; s += blockDim.x) s_acc[s] = s_win[s] = 0;
     __syncthreads();
@@ -233,7 +234,7 @@ __global__ void k_evals(const uint64_t *node_total, NodeArrays nodes, uint32_t l
             atomicAdd((unsigned long long *)&ef->evals_stage[s], s_acc[s]);
             atomicAdd((unsigned long long *)&ef->evals_alg, s_acc[s]);
         }
-        if (s_win[s]) atomicAdd((unsigned long long *)&ef->windows_stage[s], s_win[s]);
+        if (s_win[s]) atomicAdd((unsigned long long *)&windows[s], s_win[s]);
     }
 }
 
@@ -277,9 +278,9 @@ void launch_ef_build(const uint64_t *cum, const uint64_t *pos, uint64_t nb, uint
 }
 
 void launch_evals(const uint64_t *node_total, NodeArrays nodes, uint32_t leaf, uint32_t rotate, EfParams *ef,
-                  cudaStream_t st) {
+                  uint64_t *windows, cudaStream_t st) {
     use_max_smem(k_evals);
-    k_evals<<<device_sm_count() * 4, 256, 0, st>>>(node_total, nodes, leaf, rotate, ef);
+    k_evals<<<device_sm_count() * 4, 256, 0, st>>>(node_total, nodes, leaf, rotate, ef, windows);
     count_launches(1);
 }
 

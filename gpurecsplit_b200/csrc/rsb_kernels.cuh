@@ -41,6 +41,8 @@ void exclusive_scan_u32(const uint32_t *in, uint64_t *out, size_t n, ScanTmp tmp
 
 // ---- preparation (rsb_prep.cu) ----
 void launch_hash_u64(const uint64_t *keys, uint64_t n, uint64_t *out128, cudaStream_t st);
+void launch_part_first(uint64_t *keys128, uint64_t n, uint64_t nb_total, uint64_t lo, uint64_t nbp, DevStatus *status,
+                       cudaStream_t st);
 // Key i occupies bytes[offsets[i] - base, offsets[i + 1] - base).
 void launch_hash_strings(const uint8_t *bytes, const uint64_t *offsets, uint64_t n, uint64_t base, uint64_t *out128,
                          cudaStream_t st);
@@ -77,13 +79,23 @@ struct SearchCtx {
     int num_sms;
     int occupancy_pct;           // persistent kernels keep this percentage of full occupancy
 };
+// Launch schedule of one persistent search stage: candidates (seeds, or bases for rotation
+// leaves) per lane of a window, and the percentage of full occupancy its grid keeps. Any
+// valid schedule finds the same minimum seeds; only the speed differs.
+struct StageSchedule {
+    int seeds_per_lane;
+    int occupancy_pct;
+};
+// Size class of a build for the schedule table: 0 below 2^20 keys, 1 from 2^20.
+int schedule_size_class(uint64_t keys);
+bool schedule_valid(int stage, const StageSchedule &s);
+// The built-in (tuned) schedule; brute-force leaves always take 8 seeds per lane.
+StageSchedule default_schedule(int leaf, int stage, int size_class);
 void search_higher(const SearchCtx &c, int depth, cudaStream_t st);
-void search_aggr(const SearchCtx &c, int stage, cudaStream_t st);
+void search_aggr(const SearchCtx &c, int stage, const StageSchedule &s, cudaStream_t st);
 void partition_aggr(const SearchCtx &c, int stage, cudaStream_t st);
-void search_leaves(const SearchCtx &c, int stage, cudaStream_t st);
+void search_leaves(const SearchCtx &c, int stage, const StageSchedule &s, cudaStream_t st);
 uint32_t search_slots_needed(int num_sms);
-// Candidates (seeds, or bases for rotation leaves) per window of a persistent search stage.
-uint32_t window_candidates(int leaf, int stage);
 
 // ---- encoding (rsb_encode.cu) ----
 struct EfParams {
@@ -95,7 +107,6 @@ struct EfParams {
     uint64_t desc_words;       // descriptor words incl. the sentinel
     uint64_t evals_alg;
     uint64_t evals_stage[kNumStages];
-    uint64_t windows_stage[kNumStages];  // candidate windows handed out by the persistent searches
 };
 
 // Kernels launched by this library (all threads), for the launch accounting of rsb_stats.
@@ -110,8 +121,10 @@ void launch_write_rice(const uint64_t *node_base, uint64_t nbuckets, NodeArrays 
 void launch_ef_build(const uint64_t *cum, const uint64_t *pos, uint64_t nbuckets, uint64_t keys, EfParams *ef,
                      uint64_t *lower, uint64_t lower_cap, uint64_t *upper_cum, uint64_t cum_cap, uint64_t *upper_pos,
                      uint64_t pos_cap, uint64_t *jump, uint64_t jump_cap, DevStatus *status, cudaStream_t st);
+// Also adds the candidate windows handed out by the persistent searches, per stage, to
+// windows[0, kNumStages).
 void launch_evals(const uint64_t *node_total, NodeArrays nodes, uint32_t leaf, uint32_t rotate, EfParams *ef,
-                  cudaStream_t st);
+                  uint64_t *windows, cudaStream_t st);
 
 // ---- batched construction (rsb_batch.cu) ----
 void launch_set_nbuckets(const uint64_t *set_key, uint32_t nsets, uint64_t bucket_size, uint32_t *nb, cudaStream_t st);
@@ -137,6 +150,10 @@ void launch_set_ef_fill(const uint64_t *acc, const uint64_t *pos, const uint64_t
 // ---- queries (rsb_query.cu) ----
 struct MphfView;
 void launch_query_view(const MphfView &f, const uint64_t *keys128, uint64_t n, uint64_t *out, cudaStream_t st);
+// Device self-verification of a built function (RSB_VERIFY): every bucket's Elias-Fano entry
+// against acc/pos, and every key to a distinct value below n (seen: (n + 31) / 32 words).
+void launch_verify(const MphfView &f, const uint64_t *keys128, uint64_t n, const uint64_t *acc, const uint64_t *pos,
+                   uint64_t nb, uint32_t *seen, DevStatus *status, cudaStream_t st);
 bool shape_matches_kernels(const Shape &s);
 
 }  // namespace rsb

@@ -351,7 +351,32 @@ int grid_for(uint64_t n, int threads, int cap) {
     return (int)g;
 }
 
+// Part builds: the keys of buckets [lo, lo + nbp) of an nb_total-bucket function become the
+// keys of an nbp-bucket function with the same buckets. `first` of a key of bucket lo + j is
+// replaced by (j + 1) * q - 1 with q = floor((2^64 - 1) / nbp), which remap128 sends to j:
+// (j + 1) q nbp - nbp lies in [j 2^64, (j + 1) 2^64) for nbp < 2^32. The second halves, which
+// alone decide the seeds, are unchanged. A key outside the range sets RSB_ERR_BAD_ARG.
+__global__ void k_part_first(ulonglong2 *keys, uint64_t n, uint64_t nb_total, uint64_t lo, uint64_t nbp, uint64_t q,
+                             DevStatus *status) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t b = remap128(keys[i].x, nb_total);
+        if (b < lo || b - lo >= nbp) {
+            set_error(status, RSB_ERR_BAD_ARG, i);
+            continue;
+        }
+        keys[i].x = (b - lo + 1) * q - 1;
+    }
+}
+
 }  // namespace
+
+void launch_part_first(uint64_t *keys128, uint64_t n, uint64_t nb_total, uint64_t lo, uint64_t nbp, DevStatus *status,
+                       cudaStream_t st) {
+    use_max_smem(k_part_first);
+    k_part_first<<<grid_for(n, 256, device_sm_count() * 16), 256, 0, st>>>((ulonglong2 *)keys128, n, nb_total, lo, nbp,
+                                                                           ~0ull / nbp, status);
+    count_launches(1);
+}
 
 void launch_hash_u64(const uint64_t *keys, uint64_t n, uint64_t *out128, cudaStream_t st) {
     use_max_smem(k_hash_u64);

@@ -46,6 +46,10 @@ typedef enum rsb_status {
 #define RSB_KEYS_ON_DEVICE 2u  /* key pointers are device memory; otherwise host memory */
 #define RSB_DEVICE_ONLY 4u     /* keep the result on the device; the host copy is made lazily */
 #define RSB_KEEP_SEEDS 8u      /* keep the DFS seed stream for rsb_seeds() */
+#define RSB_VERIFY 16u         /* plain builds: verify the result on the device before returning - every
+                                  bucket's Elias-Fano entry decodes to its offsets (the check the
+                                  reference's debug builds run, DoubleEF.hpp:351-364) and every key maps
+                                  to a distinct value in [0, n); a failure returns RSB_ERR_INTERNAL */
 
 /* 128-bit key hash: util/Hash128.h:14-23 (hash128_t{first, second}). */
 typedef struct rsb_hash128 {
@@ -94,6 +98,18 @@ rsb_status rsb_engine_reserve(rsb_engine *engine, uint64_t keys, uint64_t bucket
  * kernels of other streams - e.g. small requests of a build service running beside a large
  * build. Results do not change; only scheduling does. */
 rsb_status rsb_engine_set_occupancy(rsb_engine *engine, uint32_t percent);
+/* Schedule of one persistent search stage (no reference counterpart: the reference's launch
+ * constants are fixed, GPURecSplit.cuh:420-425): candidates per lane of a search window and
+ * the percentage of the engine's occupancy the stage's grid keeps, for builds of `leaf_size`
+ * in size class `size_class` (0: fewer than 2^20 keys, 1: at least 2^20). `stage`: 17 upper
+ * aggregation (seeds_per_lane 8, 12 or 16), 18 lower aggregation (8, 12 or 16), 19 rotation
+ * leaves (bases per lane 4, 8 or 12); occupancy 1..100. seeds_per_lane 0 restores the
+ * built-in schedule (the table gpurecsplit_b200/tune.py measured). Every schedule finds the
+ * same minimum seeds: results never change, only speed. */
+rsb_status rsb_engine_set_schedule(rsb_engine *engine, uint32_t leaf_size, uint32_t stage, uint32_t size_class,
+                                   uint32_t seeds_per_lane, uint32_t occupancy_pct);
+rsb_status rsb_engine_get_schedule(rsb_engine *engine, uint32_t leaf_size, uint32_t stage, uint32_t size_class,
+                                   uint32_t *seeds_per_lane, uint32_t *occupancy_pct);
 
 /* ---- construction ------------------------------------------------------------------ */
 
@@ -165,6 +181,30 @@ rsb_status rsb_server_submit_hash128(rsb_server *server, const rsb_hash128 *keys
 rsb_status rsb_server_wait(rsb_server *server, uint64_t id, double timeout_s, rsb_mphf **out, rsb_request_info *info);
 /* Stops accepting requests, finishes the queued ones and releases the engines. */
 rsb_status rsb_server_destroy(rsb_server *server);
+
+/* ---- sharded construction over bucket ranges (several GPUs) ---------------------------
+ * No reference counterpart as an API: the reference builds contiguous bucket ranges in its
+ * threads and appends their Rice streams in bucket order (SIMDRecSplit.hpp:695-745). Here a
+ * range can be built on another GPU (or process) and the ranges merged into the one function
+ * the plain build makes from all keys, byte for byte. */
+
+/* Builds the part of an nbuckets_total-bucket function (nbuckets_total = ceil(n_all /
+ * bucket_size) for the n_all keys of all parts) that covers buckets [bucket_lo, bucket_hi):
+ * `keys` are exactly the keys whose bucket remap128(first, nbuckets_total) lies in the range,
+ * in any order (a key outside it returns RSB_ERR_BAD_ARG). The handle serves rsb_part_export;
+ * it is not itself a complete function. */
+rsb_status rsb_build_part_hash128(rsb_engine *engine, const rsb_hash128 *keys, uint64_t n, uint64_t nbuckets_total,
+                                  uint64_t bucket_lo, uint64_t bucket_hi, uint64_t bucket_size, uint32_t leaf_size,
+                                  uint32_t flags, rsb_mphf **out);
+/* Writes a part as bytes (its bucket range, per-bucket key and bit offsets, Rice bits) to
+ * hand to the merging process. With buf == NULL only *len is set. */
+rsb_status rsb_part_export(rsb_mphf *part, uint8_t *buf, size_t *len);
+/* Merges exported parts that tile buckets [0, nbuckets_total) in order into the complete
+ * function (host and device copies; the Elias-Fano index is built on the engine's device).
+ * `leaf_size` and RSB_ROTATE in `flags` must match the parts'. RSB_ERR_FORMAT for malformed
+ * parts, RSB_ERR_BAD_ARG for parts that do not tile one function. */
+rsb_status rsb_merge_parts(rsb_engine *engine, const uint8_t *const *parts, const size_t *lens, uint32_t nparts,
+                           uint32_t leaf_size, uint32_t flags, rsb_mphf **out);
 
 /* ---- queries and accessors --------------------------------------------------------- */
 

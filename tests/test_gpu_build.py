@@ -265,3 +265,20 @@ def test_reduced_occupancy_same_function(rsb, oracle_mod, pct):
     f = rsb.GPURecSplit(keys, bucket_size=2000, leaf_size=16, engine=eng)
     assert f.serialize() == oracle_mod.build_mphf(keys, 16, 2000).bytes.tobytes()
     eng.close()
+
+
+@pytest.mark.parametrize("leaf,b,n,kind", [(8, 100, 200_000, "hash128"), (16, 2000, 40_000, "u64"),
+                                           (12, 7, 30_000, "hash128"), (24, 2000, 500, "hash128"),
+                                           (5, 100, 0, "hash128"), (8, 100, 1, "hash128"), (10, 50, 20_000, "strings")])
+def test_verified_builds(rsb, oracle_mod, engine, leaf, b, n, kind):
+    """RSB_VERIFY: the device decodes every bucket's Elias-Fano entry and checks the bijection
+    of all keys before returning; the function is the same as without verification."""
+    if kind == "hash128":
+        keys = oracle_mod.keygen_hash128(n + leaf, n)
+    elif kind == "u64":
+        keys = oracle_mod.keygen_u64(n + leaf, n)
+    else:
+        keys = oracle_mod.keygen_strings(n + leaf, n)
+    f = rsb.GPURecSplit(keys, bucket_size=b, leaf_size=leaf, key_type=kind, engine=engine, verify=True)
+    g = rsb.GPURecSplit(keys, bucket_size=b, leaf_size=leaf, key_type=kind, engine=engine)
+    assert f.serialize() == g.serialize()

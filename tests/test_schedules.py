@@ -1,0 +1,37 @@
+"""The built-in stage schedule table (gpurecsplit_b200/csrc/rsb_schedules.inc) is the one the
+tuner measured (gpurecsplit_b200/schedules.json), and every entry is a valid schedule."""
+import json
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+INC = os.path.join(ROOT, "gpurecsplit_b200", "csrc", "rsb_schedules.inc")
+JSON = os.path.join(ROOT, "gpurecsplit_b200", "schedules.json")
+
+
+def _inc_entries():
+    rows = re.findall(r"\{(\d+), (\d+), (\d+), (\d+), (\d+)\}", open(INC).read())
+    return [tuple(int(x) for x in r) for r in rows]
+
+
+def test_table_entries_are_valid():
+    seen = set()
+    for leaf, stage, cls, s, pct in _inc_entries():
+        assert 2 <= leaf <= 24 and cls in (0, 1) and 1 <= pct <= 100
+        assert s in ((8, 12, 16) if stage in (17, 18) else (4, 8, 12)) and stage in (17, 18, 19)
+        assert (leaf, stage, cls) not in seen
+        seen.add((leaf, stage, cls))
+
+
+def test_table_matches_the_measurements():
+    if not os.path.exists(JSON):
+        pytest.skip("no tuning run recorded")
+    entries = json.load(open(JSON))["entries"]
+    want = sorted((e["leaf"], e["stage"], e["size_class"], e["seeds_per_lane"], e["occupancy_pct"]) for e in entries)
+    assert sorted(_inc_entries()) == want
+    for e in entries:
+        if "copied_from_size_class" in e:
+            continue
+        assert e["ms_best"] <= min(e["ms"].values()) + 1e-9
