@@ -116,6 +116,8 @@ def lib():
             "rsb_build_part_hash128": ([vp, vp, u64, u64, u64, u64, u64, u32, u32, pp], i32),
             "rsb_part_export": ([vp, vp, ctypes.POINTER(ctypes.c_size_t)], i32),
             "rsb_engine_set_schedule": ([vp, u32, u32, u32, u32, u32], i32),
+            "rsb_engine_set_pipeline": ([vp, u32], i32),
+            "rsb_engine_set_watchdog": ([vp, ctypes.c_double], i32),
             "rsb_engine_get_schedule": ([vp, u32, u32, u32, ctypes.POINTER(u32), ctypes.POINTER(u32)], i32),
             "rsb_merge_parts": ([vp, vp, vp, u32, u32, u32, pp], i32),
             "rsb_server_create": ([i32, u64, u32, u64, pp], i32),
@@ -171,6 +173,15 @@ class Engine:
     def set_occupancy(self, percent: int) -> None:
         """Runs the persistent search kernels at `percent` of full occupancy (rsb_engine_set_occupancy)."""
         _check(lib().rsb_engine_set_occupancy(self._h, percent), "rsb_engine_set_occupancy")
+
+    def set_pipeline(self, on: bool) -> None:
+        """Runs the aggregation and leaf searches of every build as one persistent launch with
+        device work queues (rsb_engine_set_pipeline); the functions are the same."""
+        _check(lib().rsb_engine_set_pipeline(self._h, 1 if on else 0), "rsb_engine_set_pipeline")
+
+    def set_watchdog(self, seconds: float) -> None:
+        """Upper bound on one pipeline-mode launch (rsb_engine_set_watchdog); 0: none."""
+        _check(lib().rsb_engine_set_watchdog(self._h, float(seconds)), "rsb_engine_set_watchdog")
 
     def set_schedule(self, leaf_size: int, stage: int, size_class: int, seeds_per_lane: int,
                      occupancy_pct: int = 100) -> None:

@@ -10,6 +10,8 @@
 // It replaces GPURecSplit::hash_gen (GPURecSplit.cuh:637-815), which runs the sort,
 // grouping, unpacking and encoding on the host and calls cudaDeviceReset at the end.
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <map>
@@ -83,6 +85,11 @@ struct rsb_engine {
     uint64_t budget_min = 1ull << 16;
     std::map<uint32_t, std::pair<uint32_t *, uint32_t *>> tables;  // (leaf, rotate) -> device memo, nodes
     std::map<uint32_t, StageSchedule> schedules;  // (leaf, stage, size class) -> rsb_engine_set_schedule
+    bool pipeline = false;                         // stages 17..20 in one persistent launch (rsb_engine_set_pipeline)
+    uint64_t watchdog_ns = 0;                      // bound on a pipeline launch (rsb_engine_set_watchdog), 0: none
+    DBuf<uint32_t> pq, pcounts, pactive, pclaimed;
+    DBuf<uint8_t> pblocked;
+    DBuf<uint64_t> pscratch;
     int last_seeds_per_lane[kNumStages] = {};      // schedules of the last build's stages (rsb_stats)
     DBuf<uint64_t> keys128, raw_u64, offsets, sorted, acc, node_base, scan_tmp, pos_acc, seed;
     DBuf<uint32_t> counts, node_count, lists, stage_info, sched, slots, bits, fixed_bits, nstart, nwin;
@@ -215,6 +222,26 @@ StageSchedule engine_schedule(const rsb_engine *e, uint32_t leaf, int stage, uin
     return it != e->schedules.end() ? it->second : default_schedule((int)leaf, stage, sc);
 }
 
+// After a failed pipeline-mode build: with RSB_DEBUG set in the environment, prints the
+// queue counters and, when a bounded wait gave up, the kernel's snapshot of the unfinished
+// nodes (pipe_diagnose in rsb_pipeline_impl.cuh) to stderr.
+void report_pipeline_state(rsb_engine *e, int code, uint64_t detail, cudaStream_t st) {
+    if (!e->pipeline || !e->pcounts.p || !std::getenv("RSB_DEBUG")) return;
+    uint32_t d[kPipeCounters];
+    if (cudaMemcpyAsync(d, e->pcounts.p, sizeof(d), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return;
+    std::fprintf(stderr,
+                 "rsb pipeline failed (status %d, detail %llu): why=%u tails=%u,%u,%u,%u heads=%u,%u,%u,%u "
+                 "done=%u/%u unfinished=%u active=%u seed_known=%u parent_queued=%u never_joined=%u first=%u "
+                 "stage=%u size=%u seed=%016llx first_active=%u first_windows=%u first_parent_queued=%u "
+                 "head_slots=%x,%x,%x,%x\n",
+                 code, (unsigned long long)detail, d[11], d[0], d[1], d[2], d[3], d[4], d[5], d[6], d[7], d[8], d[9],
+                 d[12], d[13], d[14], d[15], d[16], d[17], d[18] & 0xFF, d[18] >> 8,
+                 (unsigned long long)d[19] | (unsigned long long)d[20] << 32, d[21], d[22], d[23], d[24], d[25], d[26],
+                 d[27]);
+}
+
 cudaError_t enqueue_searches(rsb_engine *e, const SearchCtx &sc, const LeafTables &lt, uint64_t keys, cudaStream_t st) {
     cudaError_t err;
     const uint32_t leaf = sc.sh.leaf;
@@ -222,6 +249,27 @@ cudaError_t enqueue_searches(rsb_engine *e, const SearchCtx &sc, const LeafTable
     for (uint32_t d = 0; d < lt.max_higher_depth && d < (uint32_t)kMaxHigherDepth; ++d) {
         search_higher(sc, (int)d, st);
         if ((err = cudaEventRecord(e->ev[2 + d], st)) != cudaSuccess) return err;
+    }
+    if (e->pipeline) {
+        // one launch for stages 17..20; its time is reported as stage 17's
+        const uint64_t max_nodes = keys + 1;
+        if (ensure(e->pq, max_nodes) != RSB_OK || ensure(e->pcounts, kPipeCounters) != RSB_OK ||
+            ensure(e->pactive, max_nodes) != RSB_OK || ensure(e->pclaimed, max_nodes) != RSB_OK ||
+            ensure(e->pblocked, max_nodes) != RSB_OK || ensure(e->pscratch, keys + 1) != RSB_OK)
+            return cudaErrorMemoryAllocation;
+        if ((err = cudaMemsetAsync(sc.slots, 0xFF, sc.nslots * sizeof(uint32_t), st)) != cudaSuccess) return err;
+        const StageSchedule sa = engine_schedule(e, leaf, kStageLower, keys);
+        const StageSchedule sl = engine_schedule(e, leaf, kStageLeafRot, keys);
+        const StageSchedule aggr{sa.seeds_per_lane == 8 ? 8 : 12, sa.occupancy_pct};
+        const StageSchedule lf{sl.seeds_per_lane, 100};
+        e->last_seeds_per_lane[kStageUpper] = e->last_seeds_per_lane[kStageLower] = aggr.seeds_per_lane;
+        e->last_seeds_per_lane[kStageLeafRot] = lf.seeds_per_lane;
+        e->last_seeds_per_lane[kStageLeafBF] = 8;
+        PipeCtx p{e->pq.p, e->pcounts.p, e->pactive.p, e->pclaimed.p, e->pblocked.p, e->pscratch.p};
+        search_pipeline(sc, p, (uint32_t)max_nodes, aggr, lf, st);
+        for (int stage = kStageUpper; stage <= kStageLeafBF; ++stage)
+            if ((err = cudaEventRecord(e->ev[2 + stage], st)) != cudaSuccess) return err;
+        return cudaGetLastError();
     }
     for (int stage : {kStageUpper, kStageLower}) {
         if ((err = cudaMemsetAsync(sc.slots, 0xFF, sc.nslots * sizeof(uint32_t), st)) != cudaSuccess) return err;
@@ -409,6 +457,7 @@ rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint
     sc.budget_min = e->budget_min;
     sc.num_sms = e->num_sms;
     sc.occupancy_pct = e->occupancy_pct;
+    sc.watchdog_ns = e->watchdog_ns;
     RSB_CKH(enqueue_searches(e, sc, lt, n, st));
 
     // ---- encoding ----
@@ -436,6 +485,7 @@ rsb_status build_device(rsb_engine *e, const uint64_t *keys128, uint64_t n, uint
     RSB_CKH(cudaMemcpyAsync(windows, e->windows.p, sizeof(windows), cudaMemcpyDeviceToHost, st));
     RSB_CKH(cudaMemcpyAsync(stage_counts, e->stage_info.p, sizeof(stage_counts), cudaMemcpyDeviceToHost, st));
     RSB_CKH(cudaStreamSynchronize(st));
+    if (dst.code != 0) report_pipeline_state(e, dst.code, dst.detail, st);
     if (dst.code != 0) return fail((rsb_status)dst.code);
 
     // stats
@@ -617,6 +667,7 @@ rsb_status build_batch_device(rsb_engine *e, const uint64_t *keys128, const uint
     sc.budget_min = e->budget_min;
     sc.num_sms = e->num_sms;
     sc.occupancy_pct = e->occupancy_pct;
+    sc.watchdog_ns = e->watchdog_ns;
     RSB_CK(enqueue_searches(e, sc, lt, n, st));
     // ---- per-set encoding ----
     launch_bucket_bits(e->node_base.p, nb_total, nodes, tab, e->bits.p, e->fixed_bits.p, e->status.p, st);
@@ -658,6 +709,7 @@ rsb_status build_batch_device(rsb_engine *e, const uint64_t *keys128, const uint
         RSB_CK(cudaMemcpyAsync(wbase.data(), e->word_base.p, wbase.size() * 8, cudaMemcpyDeviceToHost, st));
     }
     RSB_CK(cudaStreamSynchronize(st));
+    if (dst.code != 0) report_pipeline_state(e, dst.code, dst.detail, st);
     if (dst.code != 0) return (rsb_status)dst.code;
     // the used part of each output array, then one function per set
     std::vector<uint64_t> hdesc(nsets ? wbase[nsets] : 0), hlower(nsets ? bases[nsets] : 0),
@@ -819,6 +871,8 @@ rsb_status rsb_engine_destroy(rsb_engine *e) {
     release(e->bits); release(e->fixed_bits); release(e->nstart); release(e->nwin); release(e->nsize);
     release(e->nstage); release(e->bytes); release(e->status); release(e->efp); release(e->windows);
     release(e->verify_seen);
+    release(e->pq); release(e->pcounts); release(e->pactive); release(e->pclaimed); release(e->pblocked);
+    release(e->pscratch);
     release(e->set_key); release(e->set_bucket); release(e->set_bits); release(e->word_base); release(e->ef_base);
     release(e->out_block); release(e->set_nb); release(e->bucket_id); release(e->set_words); release(e->ef_words);
     release(e->set_ef);
@@ -856,6 +910,18 @@ rsb_status rsb_engine_reserve(rsb_engine *e, uint64_t keys, uint64_t bucket_size
 rsb_status rsb_engine_set_occupancy(rsb_engine *e, uint32_t percent) {
     if (!e || percent == 0 || percent > 100) return RSB_ERR_BAD_ARG;
     e->occupancy_pct = (int)percent;
+    return RSB_OK;
+}
+
+rsb_status rsb_engine_set_watchdog(rsb_engine *e, double seconds) {
+    if (!e || !(seconds >= 0) || seconds > 1e6) return RSB_ERR_BAD_ARG;
+    e->watchdog_ns = (uint64_t)(seconds * 1e9);
+    return RSB_OK;
+}
+
+rsb_status rsb_engine_set_pipeline(rsb_engine *e, uint32_t on) {
+    if (!e || on > 1) return RSB_ERR_BAD_ARG;
+    e->pipeline = on != 0;
     return RSB_OK;
 }
 

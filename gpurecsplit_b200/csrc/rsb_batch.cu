@@ -123,6 +123,8 @@ __global__ void k_set_write_rice(const uint64_t *node_base, uint64_t nb_total, N
                                  const uint64_t *pos_acc, const uint32_t *fixed_bits, const uint64_t *set_bucket,
                                  uint32_t nsets, const uint64_t *word_base, const uint64_t *set_bits, uint64_t *desc,
                                  uint64_t cap_words, DevStatus *status) {
+    // A failed build writes nothing (its unfound seeds are not codes; see k_write_rice).
+    if (*(const volatile int *)&status->code) return;
     if (word_base[nsets] > cap_words) {  // would overflow the output buffer: report instead
         if (blockIdx.x == 0 && threadIdx.x == 0) set_error(status, RSB_ERR_INTERNAL, word_base[nsets]);
         return;

@@ -52,8 +52,11 @@ __global__ void k_bucket_bits(const uint64_t *node_base, uint64_t nb, NodeArrays
         uint64_t tot = 0, fx = 0;
         bool bad = false;
         for (uint64_t j = n0 + lane; j < n1; j += 32) {
-            const uint64_t x = nodes.seed[j];
-            if (x >= kSeedFailed) bad = true;
+            uint64_t x = nodes.seed[j];
+            if (x >= kSeedFailed) {  // failed or never searched: reported, and sized as 0
+                bad = true;
+                x = 0;
+            }
             const uint32_t g = tab.memo[nodes.size[j]] >> 27;
             const uint32_t u = (uint32_t)(x >> g);  // the reference keeps x >> g in a uint32 vector
             fx += g;
@@ -72,6 +75,10 @@ __global__ void k_bucket_bits(const uint64_t *node_base, uint64_t nb, NodeArrays
 __global__ void k_write_rice(const uint64_t *node_base, uint64_t nb, NodeArrays nodes, DevTables tab,
                              const uint64_t *pos_acc, const uint32_t *fixed_bits, uint64_t *desc, uint64_t cap_words,
                              EfParams *ef, DevStatus *status) {
+    // A build that already failed (a search without a seed, a duplicate key, ...) writes
+    // nothing: its seeds are not codes, and the unary part of an unfound seed would land
+    // outside the stream.
+    if (*(const volatile int *)&status->code) return;
     const uint64_t total = pos_acc[nb];
     const uint64_t words = (((total + 1 + 7) / 8) + 7 + 7) / 8;  // resize rule of appendFixed, :77
     if (words > cap_words) {

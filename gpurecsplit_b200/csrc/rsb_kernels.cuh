@@ -78,6 +78,7 @@ struct SearchCtx {
     uint64_t budget_min;
     int num_sms;
     int occupancy_pct;           // persistent kernels keep this percentage of full occupancy
+    uint64_t watchdog_ns;        // pipeline kernel: give up with RSB_ERR_TIMEOUT after this long (0: never)
 };
 // Launch schedule of one persistent search stage: candidates (seeds, or bases for rotation
 // leaves) per lane of a window, and the percentage of full occupancy its grid keeps. Any
@@ -91,6 +92,23 @@ int schedule_size_class(uint64_t keys);
 bool schedule_valid(int stage, const StageSchedule &s);
 // The built-in (tuned) schedule; brute-force leaves always take 8 seeds per lane.
 StageSchedule default_schedule(int leaf, int stage, int size_class);
+// Device state of a pipeline launch (all aggregation and leaf searches in one persistent
+// kernel with work queues; rsb_pipeline_impl.cuh).
+// counts: [0,4) reserved tails, [4,8) heads, [8] completed nodes, [9] nodes of stages 17..20;
+// when a bounded wait gives up, [10..32) describe the unfinished nodes (pipe_diagnose).
+constexpr int kPipeCounters = 32;
+struct PipeCtx {
+    uint32_t *queue;    // node ids, one queue per stage 17..20 at that stage's list offset (kEmpty = not yet written)
+    uint32_t *counts;   // kPipeCounters words, see above
+    uint32_t *active;   // per node: warps working on it
+    uint32_t *claimed;  // per node: 1 once completed
+    uint8_t *blocked;   // per node: its parent is an aggregation node (it is queued by that parent)
+    uint64_t *scratch;  // partition scratch, one word per key
+};
+// The searches of stages 17..20 in one launch (after the fanout-2 stages). Same seeds as the
+// stage kernels. max_nodes bounds the node ids.
+void search_pipeline(const SearchCtx &c, const PipeCtx &p, uint32_t max_nodes, const StageSchedule &aggr,
+                     const StageSchedule &leaf, cudaStream_t st);
 void search_higher(const SearchCtx &c, int depth, cudaStream_t st);
 void search_aggr(const SearchCtx &c, int stage, const StageSchedule &s, cudaStream_t st);
 void partition_aggr(const SearchCtx &c, int stage, cudaStream_t st);

@@ -180,6 +180,59 @@ StageSchedule default_schedule(int leaf, int stage, int size_class) {
     return {8, 100};
 }
 
+// ---- pipeline mode: set-up of the work queues --------------------------------------------
+namespace {
+// Children of aggregation nodes are queued by their parent when it completes.
+__global__ void k_pipe_mark(const SearchCtx c, PipeCtx p) {
+    const uint32_t base = c.stage_info[kNumStages + kStageUpper];
+    const uint32_t cnt = c.stage_info[kStageUpper] + c.stage_info[kStageLower];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        const uint32_t id = c.lists[base + i];  // the lists of stages 17 and 18 are adjacent
+        const uint32_t m = c.nodes.size[id];
+        const uint32_t split = c.nodes.stage[id] == kStageUpper ? c.sh.lower : c.sh.leaf;
+        const uint32_t fan = uint16_t(m + split - 1) / split;
+        uint32_t child = id + 1;
+        for (uint32_t j = 0; j < fan; ++j) {
+            const uint32_t cm = j + 1 < fan ? split : m - (fan - 1) * split;
+            if (cm <= 1) continue;
+            p.blocked[child] = 1;
+            child += c.tab.nodes[cm];
+        }
+    }
+}
+
+// Every other node of stages 17..20 is ready at the launch.
+__global__ void k_pipe_fill(const SearchCtx c, PipeCtx p) {
+    const uint32_t base = c.stage_info[kNumStages + kStageUpper];
+    const uint32_t cnt = c.stage_info[kStageUpper] + c.stage_info[kStageLower] + c.stage_info[kStageLeafRot] +
+                         c.stage_info[kStageLeafBF];
+    if (blockIdx.x == 0 && threadIdx.x == 0) p.counts[9] = cnt;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        const uint32_t id = c.lists[base + i];
+        if (p.blocked[id]) continue;
+        const uint32_t st = c.nodes.stage[id];
+        const uint32_t at = atomicAdd(&p.counts[st - kStageUpper], 1u);
+        p.queue[c.stage_info[kNumStages + st] + at] = id;
+    }
+}
+}  // namespace
+
+void search_pipeline(const SearchCtx &c, const PipeCtx &p, uint32_t max_nodes, const StageSchedule &aggr,
+                     const StageSchedule &leaf, cudaStream_t st) {
+    cudaMemsetAsync(p.queue, 0xFF, (size_t)max_nodes * sizeof(uint32_t), st);
+    cudaMemsetAsync(p.counts, 0, kPipeCounters * sizeof(uint32_t), st);
+    cudaMemsetAsync(p.active, 0, (size_t)max_nodes * sizeof(uint32_t), st);
+    cudaMemsetAsync(p.claimed, 0, (size_t)max_nodes * sizeof(uint32_t), st);
+    cudaMemsetAsync(p.blocked, 0, max_nodes, st);
+    const int g = std::max(1, std::min<int>(c.num_sms * 8, (int)((max_nodes + 255) / 256)));
+    use_max_smem(k_pipe_mark);
+    k_pipe_mark<<<g, 256, 0, st>>>(c, p);
+    use_max_smem(k_pipe_fill);
+    k_pipe_fill<<<g, 256, 0, st>>>(c, p);
+    RSB_LEAF_SWITCH(c.sh.leaf, search_impl::run_pipeline, c, p, aggr, leaf, st);
+    count_launches(3);
+}
+
 void search_higher(const SearchCtx &c, int depth, cudaStream_t st) {
     const size_t smem = kMaxBucketSize * sizeof(uint64_t);
     cudaFuncSetAttribute(k_search_higher, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -32,6 +32,26 @@ __device__ __forceinline__ uint64_t vload64(const uint64_t *p) { return *(const 
 __device__ __forceinline__ uint32_t vload32(const uint32_t *p) { return *(const volatile uint32_t *)p; }
 __device__ __forceinline__ int status_code(const DevStatus *s) { return *(const volatile int *)&s->code; }
 
+// Shared state that decides a whole warp's path (the status, a node's seed, a counter) is
+// read by lane 0 and broadcast: the lanes of a warp need not execute a load at the same
+// time, so a word that another warp writes could otherwise differ between them and split
+// the warp around its warp-wide operations.
+__device__ __forceinline__ uint64_t warp_load64(const uint64_t *a) {
+    uint64_t v = 0;
+    if ((threadIdx.x & 31) == 0) v = vload64(a);
+    return __shfl_sync(0xffffffffu, v, 0);
+}
+__device__ __forceinline__ uint32_t warp_load32(const uint32_t *a) {
+    uint32_t v = 0;
+    if ((threadIdx.x & 31) == 0) v = vload32(a);
+    return __shfl_sync(0xffffffffu, v, 0);
+}
+__device__ __forceinline__ int warp_status(const DevStatus *s) {
+    int v = 0;
+    if ((threadIdx.x & 31) == 0) v = status_code(s);
+    return __shfl_sync(0xffffffffu, v, 0);
+}
+
 // shl.b32 clamps shift amounts >= 32 to 32 (result 0), PTX ISA "shl".
 __device__ __forceinline__ uint32_t shl_clamp(uint32_t a, uint32_t b) {
     uint32_t d;
@@ -58,7 +78,15 @@ constexpr uint32_t kAbortChunk = 64;
 // candidate costs a 32-bit add and an xor before the two multiply rounds, and the few other
 // keys take the plain 64-bit form. An exactly balanced split has sum_j j * size_j, so this
 // sum is a necessary condition.
-template <int S, bool FULL>
+// A node key: from shared memory (stage kernels), or from global memory through L2 only
+// (pipeline kernel: another SM may have partitioned the keys since this SM's L1 cached them).
+template <bool L2>
+__device__ __forceinline__ uint64_t key_at(const uint64_t *sk, uint32_t i) {
+    if (L2) return __ldcg(sk + i);
+    return sk[i];
+}
+
+template <int S, bool FULL, bool L2 = false>
 __device__ __forceinline__ void moment_sums(const uint64_t *sk, uint32_t len, uint64_t bu, uint32_t mult,
                                             uint2 *pk, uint32_t *acc) {
     constexpr uint32_t kSpan = 32u * S;
@@ -70,7 +98,7 @@ __device__ __forceinline__ void moment_sums(const uint64_t *sk, uint32_t len, ui
     for (uint32_t c0 = 0; c0 < len; c0 += 32) {
         const uint32_t i = c0 + lane;
         const bool valid = i < len;
-        const uint64_t tu = (valid ? sk[i] : 0) + bu;
+        const uint64_t tu = (valid ? key_at<L2>(sk, i) : 0) + bu;
         const uint32_t lo = (uint32_t)tu, hi = (uint32_t)(tu >> 32);
         const bool fast = (lo & 0xFFFFu) <= 0x10000u - kSpan;
         const unsigned bf = __ballot_sync(0xffffffffu, valid && fast);
@@ -95,7 +123,7 @@ __device__ __forceinline__ void moment_sums(const uint64_t *sk, uint32_t len, ui
         }
     }
     for (uint32_t j = 0; j < ns; ++j) {
-        const uint64_t tu = sk[pk[kAbortChunk - 1 - j].x] + bu;
+        const uint64_t tu = key_at<L2>(sk, pk[kAbortChunk - 1 - j].x) + bu;
 #pragma unroll
         for (int s = 0; s < S; ++s) {
             const uint64_t v = tu + lane + 32u * s;

@@ -46,14 +46,14 @@ struct AggrCfg {
 };
 
 
-template <int LEAF, int STAGE, bool WIDE>
+template <int LEAF, int STAGE, bool WIDE, bool L2 = false>
 __device__ __forceinline__ bool aggr_exact(const uint64_t *sk, uint32_t m, uint32_t fan, bool full, uint64_t sx,
                                            uint32_t tlo, uint32_t thi) {
     using C = AggrCfg<LEAF, STAGE>;
     uint32_t lo = 0, hi = 0;
     if (full) {
         for (uint32_t i = 0; i < m; ++i) {
-            const uint32_t p = (hash16(sk[i] + sx) * fan) >> 16;
+            const uint32_t p = (hash16(key_at<L2>(sk, i) + sx) * fan) >> 16;
             if (WIDE) {
                 lo += shl_clamp(1u, 8 * p);
                 hi += shl_clamp(1u, 8 * p - 32);
@@ -63,7 +63,7 @@ __device__ __forceinline__ bool aggr_exact(const uint64_t *sk, uint32_t m, uint3
         }
     } else {
         for (uint32_t i = 0; i < m; ++i) {
-            const uint32_t p = ((hash16(sk[i] + sx) * m) >> 16) / C::SPLIT;
+            const uint32_t p = ((hash16(key_at<L2>(sk, i) + sx) * m) >> 16) / C::SPLIT;
             if (WIDE) {
                 lo += shl_clamp(1u, 8 * p);
                 hi += shl_clamp(1u, 8 * p - 32);
@@ -77,7 +77,7 @@ __device__ __forceinline__ bool aggr_exact(const uint64_t *sk, uint32_t m, uint3
 
 // Phase B: checks the last `take` (<= 32) queued candidates, one per lane, and merges the
 // smallest success into the node's seed. Candidates not below `best` cannot lower it.
-template <int LEAF, int STAGE>
+template <int LEAF, int STAGE, bool L2 = false>
 __device__ __forceinline__ void aggr_drain(const uint64_t *sk, uint64_t *q, uint32_t &qn, uint32_t take, uint32_t m,
                                            uint32_t fan, bool full, uint64_t seed, uint32_t tlo, uint32_t thi,
                                            uint64_t best, uint64_t *node_seed, uint32_t *found) {
@@ -87,7 +87,7 @@ __device__ __forceinline__ void aggr_drain(const uint64_t *sk, uint64_t *q, uint
     const uint64_t x = active ? q[qn - take + lane] : ~0ull;
     __syncwarp();
     bool ok = false;
-    if (active && x < best) ok = aggr_exact<LEAF, STAGE, C::WIDE>(sk, m, fan, full, seed + x, tlo, thi);
+    if (active && x < best) ok = aggr_exact<LEAF, STAGE, C::WIDE, L2>(sk, m, fan, full, seed + x, tlo, thi);
     const uint64_t v = warp_min_u64(ok ? x : ~0ull);
     if (lane == 0 && v != ~0ull) merge_seed(node_seed, v, found);
     qn -= take;
@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
     uint64_t budget = 0;
     for (;;) {
         if (node == kEmpty) {
-            if (status_code(c.status)) break;
+            if (warp_status(c.status)) break;
             uint32_t f = 0;
             if (lane == 0) f = atomicAdd(&c.sched[STAGE], 1u);
             f = __shfl_sync(0xffffffffu, f, 0);
@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
                 if (lane == 0) c.slots[gw] = node;
             } else {
                 owner = false;
-                if (vload32(found) >= count) break;  // every node of the stage has a seed
+                if (warp_load32(found) >= count) break;  // every node of the stage has a seed
                 rng = rng * 1664525u + 1013904223u;
                 node = find_help(c, rng);
                 if (node == kEmpty) break;
@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
         if (lane == 0) w = atomicAdd(&c.nodes.next_win[node], 1u);
         w = __shfl_sync(0xffffffffu, w, 0);
         const uint64_t x0 = (uint64_t)w * W;
-        uint64_t best = vload64(&c.nodes.seed[node]);
+        uint64_t best = warp_load64(&c.nodes.seed[node]);
         if (x0 >= best || x0 >= budget) {
             while (qn > 0) {
                 best = vload64(&c.nodes.seed[node]);
@@ -407,7 +407,7 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
     uint64_t budget = 0;
     for (;;) {
         if (node == kEmpty) {
-            if (status_code(c.status)) break;
+            if (warp_status(c.status)) break;
             uint32_t f = 0;
             if (lane == 0) f = atomicAdd(&c.sched[STAGE], 1u);
             f = __shfl_sync(0xffffffffu, f, 0);
@@ -417,7 +417,7 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
                 if (lane == 0) c.slots[gw] = node;
             } else {
                 owner = false;
-                if (vload32(found) >= count) break;  // every node of the stage has a seed
+                if (warp_load32(found) >= count) break;  // every node of the stage has a seed
                 rng = rng * 1664525u + 1013904223u;
                 node = find_help(c, rng);
                 if (node == kEmpty) break;
@@ -444,7 +444,7 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
         w = __shfl_sync(0xffffffffu, w, 0);
         const uint64_t x0 = (uint64_t)w * W;                   // first base (ROT) or seed of the window
         const uint64_t enc0 = ROT ? x0 * LEAF : x0;            // first encoded seed of the window
-        uint64_t best = vload64(&c.nodes.seed[node]);
+        uint64_t best = warp_load64(&c.nodes.seed[node]);
         if (enc0 >= best || enc0 >= budget) {
             if (ROT) {
                 while (qn > 0) {
@@ -523,6 +523,20 @@ void launch_persistent(K k, const SearchCtx &c, size_t smem, const StageSchedule
     cc.nslots = g * kWarpsPerCta;
     use_max_smem(k);
     k<<<g, kThreads, smem, st>>>(cc);
+}
+
+// The same for a kernel that also takes the pipeline state.
+template <typename K>
+void launch_persistent_with(K k, const SearchCtx &c, const PipeCtx &p, size_t smem, const StageSchedule &s,
+                            cudaStream_t st) {
+    if (smem) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int pct = std::max(1, c.occupancy_pct * s.occupancy_pct / 100);
+    int g = persistent_grid(k, smem, c.num_sms, kThreads, pct);
+    g = min(g, (int)(c.nslots / kWarpsPerCta));
+    SearchCtx cc = c;
+    cc.nslots = g * kWarpsPerCta;
+    use_max_smem(k);
+    k<<<g, kThreads, smem, st>>>(cc, p);
 }
 
 template <int LEAF, int STAGE, int S>

@@ -1,6 +1,6 @@
-// Aggregation and leaf searches instantiated for leaf sizes 9..14 (the leaf sizes are
+// Aggregation and leaf searches (stage kernels and the pipeline kernel) instantiated for leaf sizes 9..14 (the leaf sizes are
 // split over several files so that they compile in parallel).
-#include "rsb_search_impl.cuh"
+#include "rsb_pipeline_impl.cuh"
 
 namespace rsb {
 namespace search_impl {
@@ -23,6 +23,19 @@ template void run_leaves<13>(const SearchCtx &, int, const StageSchedule &, cuda
 template void run_aggr<14>(const SearchCtx &, int, const StageSchedule &, cudaStream_t);
 template void run_partition<14>(const SearchCtx &, int, cudaStream_t);
 template void run_leaves<14>(const SearchCtx &, int, const StageSchedule &, cudaStream_t);
+
+template void run_pipeline<9>(const SearchCtx &, const PipeCtx &, const StageSchedule &, const StageSchedule &,
+                                 cudaStream_t);
+template void run_pipeline<10>(const SearchCtx &, const PipeCtx &, const StageSchedule &, const StageSchedule &,
+                                 cudaStream_t);
+template void run_pipeline<11>(const SearchCtx &, const PipeCtx &, const StageSchedule &, const StageSchedule &,
+                                 cudaStream_t);
+template void run_pipeline<12>(const SearchCtx &, const PipeCtx &, const StageSchedule &, const StageSchedule &,
+                                 cudaStream_t);
+template void run_pipeline<13>(const SearchCtx &, const PipeCtx &, const StageSchedule &, const StageSchedule &,
+                                 cudaStream_t);
+template void run_pipeline<14>(const SearchCtx &, const PipeCtx &, const StageSchedule &, const StageSchedule &,
+                                 cudaStream_t);
 
 }  // namespace search_impl
 }  // namespace rsb

@@ -1,6 +1,6 @@
-// Aggregation and leaf searches instantiated for leaf sizes 20..24 (the leaf sizes are
+// Aggregation and leaf searches (stage kernels and the pipeline kernel) instantiated for leaf sizes 20..24 (the leaf sizes are
 // split over several files so that they compile in parallel).
-#include "rsb_search_impl.cuh"
+#include "rsb_pipeline_impl.cuh"
 
 namespace rsb {
 namespace search_impl {
@@ -20,6 +20,17 @@ template void run_leaves<23>(const SearchCtx &, int, const StageSchedule &, cuda
 template void run_aggr<24>(const SearchCtx &, int, const StageSchedule &, cudaStream_t);
 template void run_partition<24>(const SearchCtx &, int, cudaStream_t);
 template void run_leaves<24>(const SearchCtx &, int, const StageSchedule &, cudaStream_t);
+
+template void run_pipeline<20>(const SearchCtx &, const PipeCtx &, const StageSchedule &, const StageSchedule &,
+                                 cudaStream_t);
+template void run_pipeline<21>(const SearchCtx &, const PipeCtx &, const StageSchedule &, const StageSchedule &,
+                                 cudaStream_t);
+template void run_pipeline<22>(const SearchCtx &, const PipeCtx &, const StageSchedule &, const StageSchedule &,
+                                 cudaStream_t);
+template void run_pipeline<23>(const SearchCtx &, const PipeCtx &, const StageSchedule &, const StageSchedule &,
+                                 cudaStream_t);
+template void run_pipeline<24>(const SearchCtx &, const PipeCtx &, const StageSchedule &, const StageSchedule &,
+                                 cudaStream_t);
 
 }  // namespace search_impl
 }  // namespace rsb

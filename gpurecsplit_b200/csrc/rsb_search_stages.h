@@ -14,6 +14,9 @@ template <int LEAF>
 void run_partition(const SearchCtx &c, int stage, cudaStream_t st);
 template <int LEAF>
 void run_leaves(const SearchCtx &c, int stage, const StageSchedule &s, cudaStream_t st);
+template <int LEAF>
+void run_pipeline(const SearchCtx &c, const PipeCtx &p, const StageSchedule &aggr, const StageSchedule &leaf,
+                  cudaStream_t st);
 
 }  // namespace search_impl
 }  // namespace rsb

@@ -98,6 +98,15 @@ rsb_status rsb_engine_reserve(rsb_engine *engine, uint64_t keys, uint64_t bucket
  * kernels of other streams - e.g. small requests of a build service running beside a large
  * build. Results do not change; only scheduling does. */
 rsb_status rsb_engine_set_occupancy(rsb_engine *engine, uint32_t percent);
+/* Pipeline mode (no reference counterpart; off by default): the aggregation and leaf searches
+ * of every build run as one persistent launch with device work queues - a node is searched as
+ * soon as its parent has been partitioned, instead of stage after stage with a barrier
+ * between stages. The function is the same. on: 0 or 1. */
+rsb_status rsb_engine_set_pipeline(rsb_engine *engine, uint32_t on);
+/* Upper bound on one pipeline-mode launch in seconds (0, the default: none). A launch that
+ * runs longer stops and the build returns RSB_ERR_TIMEOUT; the engine stays usable. A guard
+ * for callers that prefer an error to an unexpectedly long build. */
+rsb_status rsb_engine_set_watchdog(rsb_engine *engine, double seconds);
 /* Schedule of one persistent search stage (no reference counterpart: the reference's launch
  * constants are fixed, GPURecSplit.cuh:420-425): candidates per lane of a search window and
  * the percentage of the engine's occupancy the stage's grid keeps, for builds of `leaf_size`

@@ -187,6 +187,33 @@ def test_search_budget_exhaustion_is_reported(rsb, oracle_mod):
         e.close()
 
 
+@pytest.mark.parametrize("pipeline", [False, True], ids=["stages", "pipeline"])
+def test_failed_builds_with_small_nodes_write_nothing(rsb, oracle_mod, pipeline):
+    """A build that fails once its searches are under way (here a duplicate key) leaves seeds
+    unfound. At l=2 every node has Golomb-Rice parameter 0, and the unary code of an unfound
+    seed would start one bit before its bucket's stream (bit -1 for bucket 0): the encoder
+    must write nothing, the build must report the failure, plain and batched, and the engine
+    must stay usable."""
+    e = rsb.Engine(0)
+    try:
+        e.set_pipeline(pipeline)
+        e.set_watchdog(20)
+        keys = oracle_mod.keygen_hash128(SEED + 2, 5000)
+        dup = keys.copy()
+        dup[4000] = dup[1017]  # both in the third set of the batch below
+        with pytest.raises(rsb.RSBError) as err:
+            rsb.GPURecSplit(dup, bucket_size=2, leaf_size=2, engine=e)
+        assert err.value.name == "DUPLICATE_KEY"
+        offsets = np.array([0, 1000, 1000, 5000], dtype=np.uint64)
+        with pytest.raises(rsb.RSBError) as err:
+            rsb.build_batch(dup, offsets, 2, 2, engine=e)
+        assert err.value.name == "DUPLICATE_KEY"
+        assert rsb.GPURecSplit(keys, bucket_size=2, leaf_size=2, engine=e).serialize() == \
+            oracle_mod.build_mphf(keys, 2, 2).bytes.tobytes()
+    finally:
+        e.close()
+
+
 def test_bad_arguments(rsb, engine):
     keys = np.zeros((10, 2), dtype=np.uint64)
     for leaf, b in ((1, 100), (25, 100), (8, 0)):
