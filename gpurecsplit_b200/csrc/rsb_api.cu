@@ -89,7 +89,6 @@ struct rsb_engine {
     uint64_t watchdog_ns = 0;                      // bound on a pipeline launch (rsb_engine_set_watchdog), 0: none
     DBuf<uint32_t> pq, pcounts, pactive, pclaimed;
     DBuf<uint8_t> pblocked;
-    DBuf<uint64_t> pscratch;
     int last_seeds_per_lane[kNumStages] = {};      // schedules of the last build's stages (rsb_stats)
     DBuf<uint64_t> keys128, raw_u64, offsets, sorted, acc, node_base, scan_tmp, pos_acc, seed;
     DBuf<uint32_t> counts, node_count, lists, stage_info, sched, slots, bits, fixed_bits, nstart, nwin;
@@ -255,7 +254,7 @@ cudaError_t enqueue_searches(rsb_engine *e, const SearchCtx &sc, const LeafTable
         const uint64_t max_nodes = keys + 1;
         if (ensure(e->pq, max_nodes) != RSB_OK || ensure(e->pcounts, kPipeCounters) != RSB_OK ||
             ensure(e->pactive, max_nodes) != RSB_OK || ensure(e->pclaimed, max_nodes) != RSB_OK ||
-            ensure(e->pblocked, max_nodes) != RSB_OK || ensure(e->pscratch, keys + 1) != RSB_OK)
+            ensure(e->pblocked, max_nodes) != RSB_OK)
             return cudaErrorMemoryAllocation;
         if ((err = cudaMemsetAsync(sc.slots, 0xFF, sc.nslots * sizeof(uint32_t), st)) != cudaSuccess) return err;
         const StageSchedule sa = engine_schedule(e, leaf, kStageLower, keys);
@@ -265,7 +264,7 @@ cudaError_t enqueue_searches(rsb_engine *e, const SearchCtx &sc, const LeafTable
         e->last_seeds_per_lane[kStageUpper] = e->last_seeds_per_lane[kStageLower] = aggr.seeds_per_lane;
         e->last_seeds_per_lane[kStageLeafRot] = lf.seeds_per_lane;
         e->last_seeds_per_lane[kStageLeafBF] = 8;
-        PipeCtx p{e->pq.p, e->pcounts.p, e->pactive.p, e->pclaimed.p, e->pblocked.p, e->pscratch.p};
+        PipeCtx p{e->pq.p, e->pcounts.p, e->pactive.p, e->pclaimed.p, e->pblocked.p};
         search_pipeline(sc, p, (uint32_t)max_nodes, aggr, lf, st);
         for (int stage = kStageUpper; stage <= kStageLeafBF; ++stage)
             if ((err = cudaEventRecord(e->ev[2 + stage], st)) != cudaSuccess) return err;
@@ -872,7 +871,6 @@ rsb_status rsb_engine_destroy(rsb_engine *e) {
     release(e->nstage); release(e->bytes); release(e->status); release(e->efp); release(e->windows);
     release(e->verify_seen);
     release(e->pq); release(e->pcounts); release(e->pactive); release(e->pclaimed); release(e->pblocked);
-    release(e->pscratch);
     release(e->set_key); release(e->set_bucket); release(e->set_bits); release(e->word_base); release(e->ef_base);
     release(e->out_block); release(e->set_nb); release(e->bucket_id); release(e->set_words); release(e->ef_words);
     release(e->set_ef);

@@ -103,7 +103,6 @@ struct PipeCtx {
     uint32_t *active;   // per node: warps working on it
     uint32_t *claimed;  // per node: 1 once completed
     uint8_t *blocked;   // per node: its parent is an aggregation node (it is queued by that parent)
-    uint64_t *scratch;  // partition scratch, one word per key
 };
 // The searches of stages 17..20 in one launch (after the fanout-2 stages). Same seeds as the
 // stage kernels. max_nodes bounds the node ids.

@@ -18,7 +18,9 @@
 // taken, and a warp arriving later only takes windows above it. The warp whose decrement
 // leaves the counter at zero with a seed known claims the node (a compare-and-swap on its
 // state) and completes it. The searches themselves are those of the stage kernels, so the
-// minimum seeds - and the function - are the same.
+// minimum seeds - and the function - are the same. A warp copies an aggregation node's keys
+// into its shared memory when it joins the node; the completing warp partitions from its
+// copy straight into the key array.
 //
 // Memory ordering. Every decision a whole warp takes on shared state (the status, the
 // completed-node count, a node's seed, the active count) is read by lane 0 and broadcast, so
@@ -27,19 +29,19 @@
 // decrement, so that its seed merges precede the decrement; the warp whose decrement leaves
 // the count at zero fences again and reads the seed with an atomic, so it sees every merge of
 // the warps that left before it. A warp that joins a node after its completion takes a window
-// above the node's seed and can no longer lower it.
+// above the node's seed and can no longer lower it (its copy of the keys may be read while
+// they are being partitioned; only windows above the seed are evaluated with it).
 //
 // Self-checks: a node id taken from a queue or a help slot must be a node of stages 17..20,
 // a push must stay within its stage's queue, and a partition must fill every part exactly
 // (the seed's split of the node's keys); otherwise the launch stops with RSB_ERR_INTERNAL
 // (detail: kPipeBad* | the node id or queue) without the access.
 //
-// Waits are bounded in time (%globaltimer): a warp that has found neither a queued node nor
-// one to help for kPipelineIdleNs, while nodes remain unfinished, gives up with
-// RSB_ERR_TIMEOUT; so does a warp waiting kPipelineSlotNs for a queue slot that its producer
-// has reserved but not yet written, and every warp once the launch has run for the engine's
-// watchdog bound. The first warp to give up records the state of the unfinished nodes in the
-// queue counters (pipe_diagnose) for the host to report.
+// Waits are bounded in time (%globaltimer): a warp that has found no work while no node
+// anywhere completed for kPipelineStallNs gives up with RSB_ERR_TIMEOUT, and so does every
+// warp once the launch has run for the engine's watchdog bound. The first warp to give up
+// records the state of the unfinished nodes in the queue counters (pipe_diagnose) for the
+// host to report.
 #pragma once
 
 #include "rsb_search_impl.cuh"
@@ -48,10 +50,13 @@ namespace rsb {
 
 namespace {
 
-// An idle warp is not waiting on one slow node: a node whose seed is unknown can always be
-// helped, and a node's last drains and its partition take microseconds.
-constexpr uint64_t kPipelineIdleNs = 2000000000ull;
-constexpr uint64_t kPipelineSlotNs = 1000000000ull;
+// No node completing anywhere for this long, while nodes remain, is a stall: searches are
+// bounded by their budgets and a node's drains and partition take microseconds.
+constexpr uint64_t kPipelineStallNs = 10000000000ull;
+// Help slots an idle warp scans per look, and its sleep between looks (doubling from the
+// first to the last while it stays idle).
+constexpr uint32_t kPipeHelpScan = 512;
+constexpr uint32_t kPipeIdleSleepMin = 256, kPipeIdleSleepMax = 4096;
 constexpr int kPipeQueues = 4;  // stages 17, 18, 19, 20
 // Warps that may work on one node at a time (owner and helpers): more only take windows past
 // the node's seed.
@@ -94,42 +99,74 @@ __device__ __forceinline__ bool pipe_push(const SearchCtx &c, const PipeCtx &p, 
     return true;
 }
 
-// Takes a ready node from the highest non-empty queue; kEmpty when all are empty. Called by
-// lane 0. A slot that was reserved but not yet written is waited for (bounded).
-__device__ uint32_t pipe_pop(const SearchCtx &c, const PipeCtx &p) {
+// Queue tickets. A warp takes a node by drawing a ticket - the next slot index of a queue, one
+// atomicAdd on its head - and reading that slot; a slot whose node is not pushed yet stays the
+// warp's ticket, and the warp reads it again at its next look (meanwhile it may help other
+// nodes). Every node of a stage is pushed exactly once, so a ticket below the stage's node
+// count is filled eventually and a ticket at or past it is dead. A warp draws a new ticket
+// only when it holds none for that queue and the queue's reserved tail is ahead of its head,
+// so each push costs one atomic of the warps waiting for it, not a retry of every idle warp.
+constexpr uint32_t kNoTicket = 0xFFFFFFFFu;
+constexpr uint32_t kDeadTicket = 0xFFFFFFFEu;
+
+// Takes a ready node, highest queue first; kEmpty when none is ready. Lane 0; tk holds the
+// warp's tickets.
+__device__ uint32_t pipe_pop(const SearchCtx &c, const PipeCtx &p, uint32_t (&tk)[kPipeQueues]) {
+#pragma unroll
     for (int q = 0; q < kPipeQueues; ++q) {
-        uint32_t h = vload32(&p.counts[kPipeQueues + q]);
-        while (h < vload32(&p.counts[q])) {
-            const uint32_t old = atomicCAS(&p.counts[kPipeQueues + q], h, h + 1);
-            if (old != h) {
-                h = old;
-                continue;
-            }
-            uint32_t *slot = &p.queue[c.stage_info[kNumStages + kStageUpper + q] + h];
-            uint32_t id = vload32(slot);
-            const uint64_t t0 = id == kEmpty ? globaltimer_ns() : 0;
-            while (id == kEmpty) {
-                if (globaltimer_ns() - t0 > kPipelineSlotNs) {
-                    set_error(c.status, RSB_ERR_TIMEOUT, 2);
-                    return kEmpty;
-                }
-                __nanosleep(64);
-                id = vload32(slot);
-            }
-            __threadfence();
-            return id;
+        const int st = kStageUpper + q;
+        if (tk[q] == kDeadTicket) continue;
+        if (tk[q] == kNoTicket) {
+            if (vload32(&p.counts[kPipeQueues + q]) >= vload32(&p.counts[q])) continue;
+            const uint32_t t = atomicAdd(&p.counts[kPipeQueues + q], 1u);
+            tk[q] = t < c.stage_info[st] ? t : kDeadTicket;
+            if (tk[q] == kDeadTicket) continue;
         }
+        const uint32_t id = vload32(&p.queue[c.stage_info[kNumStages + st] + tk[q]]);
+        if (id == kEmpty) continue;  // not pushed yet: the ticket stays
+        __threadfence();              // the node's keys, published before its id, are read after it
+        tk[q] = kNoTicket;
+        return id;
     }
     return kEmpty;
 }
 
-// Stable fanout-way partition of an aggregation node's keys through the scratch array, then
-// its children (DFS order: the first child follows the node, each next one follows the
-// previous child's subtree) go to their queues. The seed splits the keys exactly, so every
-// part fills its range; a partition that does not (a seed that was not the node's) writes
-// nothing outside the node, stops the launch and pushes no child.
+// Scans kPipeHelpScan help slots from `start` (four per lane per step) for a node whose seed
+// is unknown and that fewer than kPipeMaxWarpsPerNode warps work on; kEmpty if none.
+// Warp-uniform result.
+__device__ uint32_t pipe_find_help(const SearchCtx &c, const PipeCtx &p, uint32_t start) {
+    constexpr uint32_t U = 4;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t nw = min(c.nslots, gridDim.x * (uint32_t)kWarpsPerCta);
+    const uint32_t span = min(nw, kPipeHelpScan);
+    start %= nw;
+    for (uint32_t k = 0; k < span; k += 32 * U) {
+        uint32_t pick = kEmpty;
+#pragma unroll
+        for (uint32_t j = 0; j < U; ++j) {
+            const uint32_t off = k + j * 32 + lane;
+            uint32_t idx = start + off;
+            if (idx >= nw) idx -= nw;
+            const uint32_t nd = off < span ? vload32(&c.slots[idx]) : kEmpty;
+            if (pick == kEmpty && nd != kEmpty && vload64(&c.nodes.seed[nd]) == kSeedNotFound &&
+                vload32(&p.active[nd]) < kPipeMaxWarpsPerNode)
+                pick = nd;
+        }
+        const unsigned b = __ballot_sync(0xffffffffu, pick != kEmpty);
+        if (b) return __shfl_sync(0xffffffffu, pick, __ffs(b) - 1);
+    }
+    return kEmpty;
+}
+
+// Stable fanout-way partition of an aggregation node's keys, from the completing warp's
+// shared-memory copy (sk) into the key array, then its children (DFS order: the first child
+// follows the node, each next one follows the previous child's subtree) go to their queues.
+// The seed splits the keys exactly, so every part fills its range; a partition that does not
+// (a seed that was not the node's) writes nothing outside the node, stops the launch and
+// pushes no child.
 template <int LEAF, int STAGE>
-__device__ void pipe_complete_aggr(const SearchCtx &c, const PipeCtx &p, uint32_t id, uint64_t x) {
+__device__ void pipe_complete_aggr(const SearchCtx &c, const PipeCtx &p, uint32_t id, uint64_t x,
+                                   const uint64_t *sk) {
     using C = AggrCfg<LEAF, STAGE>;
     const int lane = threadIdx.x & 31;
     const uint32_t start = c.nodes.start[id];
@@ -143,7 +180,7 @@ __device__ void pipe_complete_aggr(const SearchCtx &c, const PipeCtx &p, uint32_
     for (uint32_t c0 = 0; c0 < m; c0 += 32) {
         const uint32_t i = c0 + lane;
         const bool valid = i < m;
-        const uint64_t k = valid ? __ldcg(&c.keys[start + i]) : 0;
+        const uint64_t k = valid ? sk[i] : 0;
         const uint32_t part = valid ? remap16(k + sx, m) / C::SPLIT : 0xFFu;
         uint32_t dst = 0xFFFFFFFFu;
 #pragma unroll
@@ -154,7 +191,7 @@ __device__ void pipe_complete_aggr(const SearchCtx &c, const PipeCtx &p, uint32_
                 cur[j] += __popc(b);
             }
         }
-        if (valid && dst < m) __stcg(&p.scratch[start + dst], k);
+        if (valid && dst < m) __stcg(&c.keys[start + dst], k);
         bad |= valid && dst >= m;
     }
 #pragma unroll
@@ -164,9 +201,6 @@ __device__ void pipe_complete_aggr(const SearchCtx &c, const PipeCtx &p, uint32_
         if (lane == 0) set_error(c.status, RSB_ERR_INTERNAL, kPipeBadSplit | id);
         return;
     }
-    __threadfence();
-    __syncwarp();
-    for (uint32_t i = lane; i < m; i += 32) __stcg(&c.keys[start + i], __ldcg(&p.scratch[start + i]));
     __threadfence();  // every lane's keys before lane 0 publishes the children
     __syncwarp();
     if (lane == 0) {
@@ -212,7 +246,7 @@ __device__ __forceinline__ void aggr_flush(const SearchCtx &c, PipeNode &s, cons
     const uint64_t seed = start_seed(C::SEED_INDEX);
     while (s.qn > 0) {
         const uint64_t best = vload64(&c.nodes.seed[s.id]);
-        aggr_drain<LEAF, STAGE, true>(sk, q, s.qn, min(s.qn, 32u), s.m, s.fan, s.full, seed, s.tlo, s.thi, best,
+        aggr_drain<LEAF, STAGE>(sk, q, s.qn, min(s.qn, 32u), s.m, s.fan, s.full, seed, s.tlo, s.thi, best,
                                       &c.nodes.seed[s.id], found);
     }
 }
@@ -241,8 +275,8 @@ __device__ bool aggr_window(const SearchCtx &c, PipeNode &s, const uint64_t *sk,
     for (int k = 0; k < S; ++k) cnt[k] = s.full ? kAccF0 : 0u;
     for (uint32_t i0 = 0; i0 < s.m; i0 += kAbortChunk) {
         const uint32_t len = min(kAbortChunk, s.m - i0);
-        if (s.full) moment_sums<S, true, true>(sk + i0, len, seed + x0, s.fan, pk, cnt);
-        else moment_sums<S, false, true>(sk + i0, len, seed + x0, s.mult, pk, cnt);
+        if (s.full) moment_sums<S, true>(sk + i0, len, seed + x0, s.fan, pk, cnt);
+        else moment_sums<S, false>(sk + i0, len, seed + x0, s.mult, pk, cnt);
         if (i0 + len < s.m) {
             uint64_t b = 0;
             if (lane == 0) b = vload64(&c.nodes.seed[s.id]);
@@ -259,7 +293,7 @@ __device__ bool aggr_window(const SearchCtx &c, PipeNode &s, const uint64_t *sk,
     __syncwarp();
     while (s.qn >= 32) {
         best = vload64(&c.nodes.seed[s.id]);
-        aggr_drain<LEAF, STAGE, true>(sk, q, s.qn, 32u, s.m, s.fan, s.full, seed, s.tlo, s.thi, best,
+        aggr_drain<LEAF, STAGE>(sk, q, s.qn, 32u, s.m, s.fan, s.full, seed, s.tlo, s.thi, best,
                                       &c.nodes.seed[s.id], found);
     }
     return true;
@@ -331,17 +365,18 @@ __device__ bool leaf_window(const SearchCtx &c, PipeNode &s, const uint64_t *sk,
 }
 
 // Per-warp shared memory of the pipeline kernel: the larger of the aggregation layout (the
-// phase-B queue of the larger window and the per-key terms) and the leaf layout.
+// keys of the largest aggregation node, the phase-B queue of the window and the per-key
+// terms) and the leaf layout.
 template <int LEAF, int SA, int SL>
 __host__ __device__ constexpr size_t pipe_warp_bytes() {
-    constexpr size_t aggr = 8 * (size_t)(32 + 32 * SA) + 8 * (size_t)kAbortChunk;
+    constexpr size_t aggr = 8 * (size_t)(upper_of(LEAF) + 32 + 32 * SA) + 8 * (size_t)kAbortChunk;
     constexpr size_t leaf = leaf_warp_bytes<LEAF, true, SL>() + 8 * LEAF;
     return aggr > leaf ? aggr : leaf;
 }
 
 // Called by every warp that leaves the launch on RSB_ERR_TIMEOUT; the first records, in
 // counts[10..28), a snapshot of the nodes of stages 17..20 that are not complete:
-//   [10] 1 once recorded  [11] the status detail (1 idle, 2 queue slot, 3 watchdog)
+//   [10] 1 once recorded  [11] the status detail (1 stall, 3 watchdog)
 //   [12] unfinished nodes, of them [13] with warps active, [14] with a seed known,
 //   [15] queued by their parent, [16] with no window handed out yet
 //   [17] the first unfinished node, [18] its stage | size << 8, [19] [20] its seed (low and
@@ -405,8 +440,9 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(SearchCtx c, PipeCtx p) {
     extern __shared__ uint64_t smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint8_t *wbase = reinterpret_cast<uint8_t *>(smem) + warp * pipe_warp_bytes<LEAF, SA, SL>();
-    // aggregation layout: phase-B queue, per-key terms
-    uint64_t *aq = reinterpret_cast<uint64_t *>(wbase);
+    // aggregation layout: the node's keys, phase-B queue, per-key terms
+    uint64_t *ask = reinterpret_cast<uint64_t *>(wbase);
+    uint64_t *aq = ask + upper_of(LEAF);
     uint2 *apk = reinterpret_cast<uint2 *>(aq + 32 + 32 * SA);
     // leaf layout: keys, per-key terms, phase-A queue (bases, masks), rotation queue (bases, masks)
     uint64_t *lsk = reinterpret_cast<uint64_t *>(wbase);
@@ -417,7 +453,13 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(SearchCtx c, PipeCtx p) {
     uint2 *cm = reinterpret_cast<uint2 *>(cb + kRotQueueCap);
     const uint32_t gw = blockIdx.x * kWarpsPerCta + warp;
     uint32_t rng = gw * 2654435761u + 4242u;
-    uint64_t idle_since = 0;  // lane 0: when the warp last ran out of work (0: it has work)
+    // lane 0: queue tickets; the completed-node count seen and when it last changed while
+    // this warp was idle (0: not idle); the idle sleep
+    uint32_t tk[kPipeQueues];
+#pragma unroll
+    for (int q = 0; q < kPipeQueues; ++q) tk[q] = kNoTicket;
+    uint32_t seen_done = 0, sleep_ns = kPipeIdleSleepMin;
+    uint64_t idle_since = 0;
     const uint64_t t_start = globaltimer_ns();
     PipeNode s{};
     s.id = kEmpty;
@@ -434,36 +476,39 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(SearchCtx c, PipeCtx p) {
             uint32_t id = kEmpty, stop = 0;
             if (lane == 0) {
                 stop = status_code(c.status) != 0;
-                if (!stop) id = pipe_pop(c, p);
+                if (!stop) id = pipe_pop(c, p, tk);
             }
             if (__shfl_sync(0xffffffffu, stop, 0)) break;
             id = __shfl_sync(0xffffffffu, id, 0);
             s.owner = id != kEmpty;
             if (id == kEmpty) {
-                uint32_t done = 0;
-                if (lane == 0) done = vload32(&p.counts[2 * kPipeQueues]) >= p.counts[2 * kPipeQueues + 1];
+                uint32_t done = 0, now_done = 0;
+                if (lane == 0) {
+                    now_done = vload32(&p.counts[2 * kPipeQueues]);
+                    done = now_done >= p.counts[2 * kPipeQueues + 1];
+                }
                 if (__shfl_sync(0xffffffffu, done, 0)) break;  // every node is complete
                 rng = rng * 1664525u + 1013904223u;
-                id = find_help(c, rng);
-                if (id != kEmpty) {
-                    uint32_t crowded = 0;
-                    if (lane == 0) crowded = vload32(&p.active[id]) >= kPipeMaxWarpsPerNode;
-                    if (__shfl_sync(0xffffffffu, crowded, 0)) id = kEmpty;
-                }
+                id = pipe_find_help(c, p, rng);
                 if (id == kEmpty) {
                     uint32_t give_up = 0;
                     if (lane == 0) {
                         const uint64_t now = globaltimer_ns();
-                        if (idle_since == 0) idle_since = now;
-                        give_up = now - idle_since > kPipelineIdleNs;
+                        if (idle_since == 0 || now_done != seen_done) {
+                            idle_since = now;
+                            seen_done = now_done;
+                        }
+                        give_up = now - idle_since > kPipelineStallNs;
                         if (give_up) set_error(c.status, RSB_ERR_TIMEOUT, 1);
                     }
                     if (__shfl_sync(0xffffffffu, give_up, 0)) break;
-                    __nanosleep(1000);
+                    __nanosleep(sleep_ns);
+                    sleep_ns = min(2 * sleep_ns, kPipeIdleSleepMax);
                     continue;
                 }
             }
             idle_since = 0;
+            sleep_ns = kPipeIdleSleepMin;
             uint32_t ok = 0;
             if (lane == 0) {
                 ok = pipe_node_ok(c, id);
@@ -482,10 +527,12 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(SearchCtx c, PipeCtx p) {
             s.m = c.nodes.size[id];
             s.budget = budget_for(c, s.m);
             s.qn = s.cn = 0;
-            if (s.stage == kStageUpper) {
-                aggr_setup<LEAF, kStageUpper>(c, s);
-            } else if (s.stage == kStageLower) {
-                aggr_setup<LEAF, kStageLower>(c, s);
+            if (s.stage == kStageUpper || s.stage == kStageLower) {
+                const uint32_t start = c.nodes.start[id];
+                for (uint32_t i = lane; i < s.m; i += 32) ask[i] = __ldcg(&c.keys[start + i]);
+                __syncwarp();
+                if (s.stage == kStageUpper) aggr_setup<LEAF, kStageUpper>(c, s);
+                else aggr_setup<LEAF, kStageLower>(c, s);
             } else {
                 const uint32_t start = c.nodes.start[id];
                 const uint64_t k = lane < (int)s.m ? __ldcg(&c.keys[start + lane]) : 0;
@@ -501,12 +548,11 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(SearchCtx c, PipeCtx p) {
                 __syncwarp();
             }
         }
-        const uint64_t *gk = c.keys + c.nodes.start[s.id];  // aggregation nodes read their keys in place
         uint32_t *found = &c.sched[kNumStages + s.stage];
         bool stay;
         switch (s.stage) {
-            case kStageUpper: stay = aggr_window<LEAF, kStageUpper, SA>(c, s, gk, aq, apk, found); break;
-            case kStageLower: stay = aggr_window<LEAF, kStageLower, SA>(c, s, gk, aq, apk, found); break;
+            case kStageUpper: stay = aggr_window<LEAF, kStageUpper, SA>(c, s, ask, aq, apk, found); break;
+            case kStageLower: stay = aggr_window<LEAF, kStageLower, SA>(c, s, ask, aq, apk, found); break;
             case kStageLeafRot: stay = leaf_window<LEAF, true, SL>(c, s, lsk, lpk, qb, qm, cb, cm, found); break;
             default: stay = leaf_window<LEAF, false, 8>(c, s, lsk, lpk, qb, qm, cb, cm, found); break;
         }
@@ -532,9 +578,9 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(SearchCtx c, PipeCtx p) {
                 if (x >= kSeedFailed) {
                     if (lane == 0) set_error(c.status, RSB_ERR_SEARCH_BUDGET, s.id);
                 } else if (s.stage == kStageUpper) {
-                    pipe_complete_aggr<LEAF, kStageUpper>(c, p, s.id, x);
+                    pipe_complete_aggr<LEAF, kStageUpper>(c, p, s.id, x, ask);
                 } else if (s.stage == kStageLower) {
-                    pipe_complete_aggr<LEAF, kStageLower>(c, p, s.id, x);
+                    pipe_complete_aggr<LEAF, kStageLower>(c, p, s.id, x, ask);
                 }
                 if (lane == 0) atomicAdd(&p.counts[2 * kPipeQueues], 1u);
             }

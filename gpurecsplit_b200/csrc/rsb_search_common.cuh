@@ -78,15 +78,7 @@ constexpr uint32_t kAbortChunk = 64;
 // candidate costs a 32-bit add and an xor before the two multiply rounds, and the few other
 // keys take the plain 64-bit form. An exactly balanced split has sum_j j * size_j, so this
 // sum is a necessary condition.
-// A node key: from shared memory (stage kernels), or from global memory through L2 only
-// (pipeline kernel: another SM may have partitioned the keys since this SM's L1 cached them).
-template <bool L2>
-__device__ __forceinline__ uint64_t key_at(const uint64_t *sk, uint32_t i) {
-    if (L2) return __ldcg(sk + i);
-    return sk[i];
-}
-
-template <int S, bool FULL, bool L2 = false>
+template <int S, bool FULL>
 __device__ __forceinline__ void moment_sums(const uint64_t *sk, uint32_t len, uint64_t bu, uint32_t mult,
                                             uint2 *pk, uint32_t *acc) {
     constexpr uint32_t kSpan = 32u * S;
@@ -98,7 +90,7 @@ __device__ __forceinline__ void moment_sums(const uint64_t *sk, uint32_t len, ui
     for (uint32_t c0 = 0; c0 < len; c0 += 32) {
         const uint32_t i = c0 + lane;
         const bool valid = i < len;
-        const uint64_t tu = (valid ? key_at<L2>(sk, i) : 0) + bu;
+        const uint64_t tu = (valid ? sk[i] : 0) + bu;
         const uint32_t lo = (uint32_t)tu, hi = (uint32_t)(tu >> 32);
         const bool fast = (lo & 0xFFFFu) <= 0x10000u - kSpan;
         const unsigned bf = __ballot_sync(0xffffffffu, valid && fast);
@@ -123,7 +115,7 @@ __device__ __forceinline__ void moment_sums(const uint64_t *sk, uint32_t len, ui
         }
     }
     for (uint32_t j = 0; j < ns; ++j) {
-        const uint64_t tu = key_at<L2>(sk, pk[kAbortChunk - 1 - j].x) + bu;
+        const uint64_t tu = sk[pk[kAbortChunk - 1 - j].x] + bu;
 #pragma unroll
         for (int s = 0; s < S; ++s) {
             const uint64_t v = tu + lane + 32u * s;

@@ -46,14 +46,14 @@ struct AggrCfg {
 };
 
 
-template <int LEAF, int STAGE, bool WIDE, bool L2 = false>
+template <int LEAF, int STAGE, bool WIDE>
 __device__ __forceinline__ bool aggr_exact(const uint64_t *sk, uint32_t m, uint32_t fan, bool full, uint64_t sx,
                                            uint32_t tlo, uint32_t thi) {
     using C = AggrCfg<LEAF, STAGE>;
     uint32_t lo = 0, hi = 0;
     if (full) {
         for (uint32_t i = 0; i < m; ++i) {
-            const uint32_t p = (hash16(key_at<L2>(sk, i) + sx) * fan) >> 16;
+            const uint32_t p = (hash16(sk[i] + sx) * fan) >> 16;
             if (WIDE) {
                 lo += shl_clamp(1u, 8 * p);
                 hi += shl_clamp(1u, 8 * p - 32);
@@ -63,7 +63,7 @@ __device__ __forceinline__ bool aggr_exact(const uint64_t *sk, uint32_t m, uint3
         }
     } else {
         for (uint32_t i = 0; i < m; ++i) {
-            const uint32_t p = ((hash16(key_at<L2>(sk, i) + sx) * m) >> 16) / C::SPLIT;
+            const uint32_t p = ((hash16(sk[i] + sx) * m) >> 16) / C::SPLIT;
             if (WIDE) {
                 lo += shl_clamp(1u, 8 * p);
                 hi += shl_clamp(1u, 8 * p - 32);
@@ -77,7 +77,7 @@ __device__ __forceinline__ bool aggr_exact(const uint64_t *sk, uint32_t m, uint3
 
 // Phase B: checks the last `take` (<= 32) queued candidates, one per lane, and merges the
 // smallest success into the node's seed. Candidates not below `best` cannot lower it.
-template <int LEAF, int STAGE, bool L2 = false>
+template <int LEAF, int STAGE>
 __device__ __forceinline__ void aggr_drain(const uint64_t *sk, uint64_t *q, uint32_t &qn, uint32_t take, uint32_t m,
                                            uint32_t fan, bool full, uint64_t seed, uint32_t tlo, uint32_t thi,
                                            uint64_t best, uint64_t *node_seed, uint32_t *found) {
@@ -87,7 +87,7 @@ __device__ __forceinline__ void aggr_drain(const uint64_t *sk, uint64_t *q, uint
     const uint64_t x = active ? q[qn - take + lane] : ~0ull;
     __syncwarp();
     bool ok = false;
-    if (active && x < best) ok = aggr_exact<LEAF, STAGE, C::WIDE, L2>(sk, m, fan, full, seed + x, tlo, thi);
+    if (active && x < best) ok = aggr_exact<LEAF, STAGE, C::WIDE>(sk, m, fan, full, seed + x, tlo, thi);
     const uint64_t v = warp_min_u64(ok ? x : ~0ull);
     if (lane == 0 && v != ~0ull) merge_seed(node_seed, v, found);
     qn -= take;
