@@ -25,7 +25,7 @@ contiguous bucket ranges, so the timed steps together build the whole workload o
 
 Other modes (one JSON line each): `--mode batch` (many key sets in one pipeline vs
 back-to-back plain builds), `--mode serve` (continuous batching of string requests),
-`--mode c1` and `--mode c3`.
+`--mode c1`, `--mode c3` and `--mode pipeline` (stage kernels against pipeline mode).
 
 Multi-GPU (torchrun): every rank builds its own 5M-key set (weak scaling, no data-path
 collective); the step time is the max over ranks.
@@ -834,6 +834,61 @@ def measure_serve(requests: int = 100, max_keys: int = 10_000_000, hbm_budget: i
     }
 
 
+def measure_pipeline(reps: int = 3) -> dict:
+    """Stage kernels against pipeline mode (rsb_engine_set_pipeline) on the same builds: the
+    device time of each build (CUDA events around the public call with device-resident keys,
+    best of `reps`) and whether both modes serialize to the same bytes."""
+    import torch
+    import gpurecsplit_b200 as rsb
+    torch.cuda.set_device(0)
+    st = torch.cuda.current_stream()
+    cases = [("u64 n=5M l=16 b=2000", 5_000_000, 16, 2000, 42), ("u64 n=1M l=12 b=1000", 1_000_000, 12, 1000, 42),
+             ("u64 n=1M l=8 b=100", 1_000_000, 8, 100, 42), ("u64 n=200k l=20 b=2000", 200_000, 20, 2000, 43)]
+
+    def best_ms(fn):
+        out = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            r = fn()
+            b.record(st)
+            b.synchronize()
+            out.append(a.elapsed_time(b))
+            for f in (r[0] if isinstance(r, tuple) else [r]):
+                f.close()
+        return round(min(out), 3)
+
+    rows = {}
+    for pipe in (False, True):
+        e = rsb.Engine(0, st.cuda_stream)
+        e.set_pipeline(pipe)
+        for name, n, leaf, b, seed in cases:
+            keys = torch.from_numpy(splitmix64_keys(seed, n).view(np.int64)).cuda()
+            torch.cuda.synchronize()
+            fn = (lambda k=keys, n=n, b=b, leaf=leaf:
+                  rsb.GPURecSplit.from_device(k.data_ptr(), n, b, leaf, key_type="u64", engine=e, device_only=True))
+            f = fn()
+            blob = f.serialize()
+            f.close()
+            row = rows.setdefault(name, {})
+            row["pipeline_ms" if pipe else "stages_ms"] = best_ms(fn)
+            row["sha256_" + ("pipeline" if pipe else "stages")] = hashlib.sha256(blob).hexdigest()
+            del keys
+        k, off = batch_workload(1000)
+        d = torch.from_numpy(k.view(np.int64)).cuda()
+        torch.cuda.synchronize()
+        fn = lambda: rsb.build_batch(d.data_ptr(), off, 1000, 12, key_type="u64", engine=e, keys_on_device=True)
+        row = rows.setdefault("1000 sets (%d u64 keys) l=12 b=1000" % int(off[-1]), {})
+        row["pipeline_ms" if pipe else "stages_ms"] = best_ms(fn)
+        del d
+        e.close()
+    for row in rows.values():
+        if "sha256_stages" in row:
+            row["identical"] = row.pop("sha256_stages") == row.pop("sha256_pipeline")
+    return {"mode": "pipeline", "unit": "ms", "workloads": rows}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -843,7 +898,7 @@ def main() -> None:
     ap.add_argument("--n", type=int, default=N_KEYS)
     ap.add_argument("--cpu-fraction", type=int, default=5, help="CPU baseline sample: 1/N of the workload's buckets")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="plain", choices=["plain", "batch", "serve", "c1", "c3"])
+    ap.add_argument("--mode", default="plain", choices=["plain", "batch", "serve", "c1", "c3", "pipeline"])
     ap.add_argument("--sets", type=int, default=1000)
     ap.add_argument("--requests", type=int, default=100)
     ap.add_argument("--max-keys", type=int, default=10_000_000)
@@ -854,6 +909,9 @@ def main() -> None:
     args = ap.parse_args()
     if args.mode == "batch":
         print(json.dumps(measure_batch(args.sets)), flush=True)
+        return
+    if args.mode == "pipeline":
+        print(json.dumps(measure_pipeline()), flush=True)
         return
     if args.mode == "serve":
         print(json.dumps(measure_serve(args.requests, args.max_keys, args.hbm_budget, args.inflight, args.load)),
