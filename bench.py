@@ -25,7 +25,8 @@ contiguous bucket ranges, so the timed steps together build the whole workload o
 
 Other modes (one JSON line each): `--mode batch` (many key sets in one pipeline vs
 back-to-back plain builds), `--mode serve` (continuous batching of string requests),
-`--mode c1`, `--mode c3` and `--mode pipeline` (stage kernels against pipeline mode).
+`--mode c1`, `--mode c3`, `--mode pipeline` (stage kernels against pipeline mode) and
+`--mode build` (plain builds of a chosen size, for profiling).
 
 Multi-GPU (torchrun): every rank builds its own 5M-key set (weak scaling, no data-path
 collective); the step time is the max over ranks.
@@ -889,6 +890,24 @@ def measure_pipeline(reps: int = 3) -> dict:
     return {"mode": "pipeline", "unit": "ms", "workloads": rows}
 
 
+def measure_builds(n: int, leaf: int, bucket: int, builds: int) -> dict:
+    """`builds` plain builds of n splitmix64 u64 keys (seed 42) on one engine, for profiling
+    the search kernels on a chosen size: the per-stage evaluations, times and windows of the
+    last build."""
+    import gpurecsplit_b200 as rsb
+    e = rsb.Engine(0)
+    keys = splitmix64_keys(42, n)
+    st = None
+    for _ in range(builds):
+        f = rsb.GPURecSplit(keys, bucket_size=bucket, leaf_size=leaf, key_type="u64", engine=e)
+        st = f.stats()
+        f.close()
+    e.close()
+    stages = {s: {"evals": int(st["evals_stage"][s]), "ms": round(st["ms_search"][s], 3),
+                  "windows": int(st["windows_stage"][s])} for s in range(17, 21)}
+    return {"mode": "build", "n": n, "leaf": leaf, "bucket": bucket, "builds": builds, "stages": stages}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -898,8 +917,11 @@ def main() -> None:
     ap.add_argument("--n", type=int, default=N_KEYS)
     ap.add_argument("--cpu-fraction", type=int, default=5, help="CPU baseline sample: 1/N of the workload's buckets")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="plain", choices=["plain", "batch", "serve", "c1", "c3", "pipeline"])
+    ap.add_argument("--mode", default="plain", choices=["plain", "batch", "serve", "c1", "c3", "pipeline", "build"])
     ap.add_argument("--sets", type=int, default=1000)
+    ap.add_argument("--leaf", type=int, default=16, help="--mode build: leaf size")
+    ap.add_argument("--bucket", type=int, default=2000, help="--mode build: bucket size")
+    ap.add_argument("--builds", type=int, default=2, help="--mode build: builds on one engine")
     ap.add_argument("--requests", type=int, default=100)
     ap.add_argument("--max-keys", type=int, default=10_000_000)
     ap.add_argument("--hbm-budget", type=int, default=32 << 30)
@@ -909,6 +931,9 @@ def main() -> None:
     args = ap.parse_args()
     if args.mode == "batch":
         print(json.dumps(measure_batch(args.sets)), flush=True)
+        return
+    if args.mode == "build":
+        print(json.dumps(measure_builds(args.n, args.leaf, args.bucket, args.builds)), flush=True)
         return
     if args.mode == "pipeline":
         print(json.dumps(measure_pipeline()), flush=True)

@@ -217,7 +217,7 @@ __device__ void pipe_complete_aggr(const SearchCtx &c, const PipeCtx &p, uint32_
 
 // Per-node search state of a warp.
 struct PipeNode {
-    uint32_t id, stage, m, fan, tlo, thi, t1, mult, nl, qn, cn;
+    uint32_t id, stage, m, fan, tlo, thi, t1, mult, nl, qn, keep, ckeep;
     bool full, owner;
     uint64_t budget;
 };
@@ -238,20 +238,8 @@ __device__ __forceinline__ void aggr_setup(const SearchCtx &c, PipeNode &s) {
     for (uint32_t j = 1; j < s.fan; ++j) s.t1 += j * (j + 1 < s.fan ? C::SPLIT : s.m - (s.fan - 1) * C::SPLIT);
 }
 
-// Drains an aggregation node's phase-B queue (q) completely.
-template <int LEAF, int STAGE>
-__device__ __forceinline__ void aggr_flush(const SearchCtx &c, PipeNode &s, const uint64_t *sk, uint64_t *q,
-                                           uint32_t *found) {
-    using C = AggrCfg<LEAF, STAGE>;
-    const uint64_t seed = start_seed(C::SEED_INDEX);
-    while (s.qn > 0) {
-        const uint64_t best = vload64(&c.nodes.seed[s.id]);
-        aggr_drain<LEAF, STAGE>(sk, q, s.qn, min(s.qn, 32u), s.m, s.fan, s.full, seed, s.tlo, s.thi, best,
-                                      &c.nodes.seed[s.id], found);
-    }
-}
-
-// One window of an aggregation node: returns false when the warp leaves the node.
+// One window of an aggregation node (phase A, then phase B of its survivors): returns false
+// when the warp leaves the node.
 template <int LEAF, int STAGE, int S>
 __device__ bool aggr_window(const SearchCtx &c, PipeNode &s, const uint64_t *sk, uint64_t *q, uint2 *pk,
                             uint32_t *found) {
@@ -264,10 +252,10 @@ __device__ bool aggr_window(const SearchCtx &c, PipeNode &s, const uint64_t *sk,
     if (lane == 0) w = atomicAdd(&c.nodes.next_win[s.id], 1u);
     w = __shfl_sync(0xffffffffu, w, 0);
     const uint64_t x0 = (uint64_t)w * W;
-    uint64_t best = warp_load64(&c.nodes.seed[s.id]);
+    const uint64_t best = warp_load64(&c.nodes.seed[s.id]);
     if (x0 >= best || x0 >= s.budget) {
-        aggr_flush<LEAF, STAGE>(c, s, sk, q, found);
-        if (x0 < vload64(&c.nodes.seed[s.id]) && lane == 0) merge_seed(&c.nodes.seed[s.id], kSeedFailed, found);
+        aggr_phase_b<LEAF, STAGE>(sk, q, s.qn, 0, s.m, s.fan, s.full, seed, s.tlo, s.thi, &c.nodes.seed[s.id], found);
+        if (x0 < warp_load64(&c.nodes.seed[s.id]) && lane == 0) merge_seed(&c.nodes.seed[s.id], kSeedFailed, found);
         return false;
     }
     uint32_t cnt[S];
@@ -291,11 +279,9 @@ __device__ bool aggr_window(const SearchCtx &c, PipeNode &s, const uint64_t *sk,
         s.qn += __popc(b);
     }
     __syncwarp();
-    while (s.qn >= 32) {
-        best = vload64(&c.nodes.seed[s.id]);
-        aggr_drain<LEAF, STAGE>(sk, q, s.qn, 32u, s.m, s.fan, s.full, seed, s.tlo, s.thi, best,
-                                      &c.nodes.seed[s.id], found);
-    }
+    aggr_phase_b<LEAF, STAGE>(sk, q, s.qn, s.keep, s.m, s.fan, s.full, seed, s.tlo, s.thi, &c.nodes.seed[s.id],
+                              found);
+    __syncwarp();  // q is appended to by the next window
     return true;
 }
 
@@ -314,14 +300,8 @@ __device__ bool leaf_window(const SearchCtx &c, PipeNode &s, const uint64_t *sk,
     const uint64_t enc0 = ROT ? x0 * LEAF : x0;
     const uint64_t best = warp_load64(node_seed);
     if (enc0 >= best || enc0 >= s.budget) {
-        if (ROT) {
-            while (s.qn > 0) {
-                leaf_drain<LEAF>(sk, s.nl, qb, qm, s.qn, min(s.qn, 32u), seed, vload64(node_seed), cb, cm, s.cn);
-                while (s.cn >= 32) rot_drain<LEAF>(cb, cm, s.cn, 32u, vload64(node_seed), node_seed, found);
-            }
-            while (s.cn > 0) rot_drain<LEAF>(cb, cm, s.cn, min(s.cn, 32u), vload64(node_seed), node_seed, found);
-        }
-        if (enc0 < vload64(node_seed) && lane == 0) merge_seed(node_seed, kSeedFailed, found);
+        if (ROT) leaf_phase_bc<LEAF>(sk, s.nl, qb, qm, s.qn, 0, s.ckeep, seed, cb, cm, node_seed, found);
+        if (enc0 < warp_load64(node_seed) && lane == 0) merge_seed(node_seed, kSeedFailed, found);
         return false;
     }
     if (ROT) {
@@ -343,11 +323,8 @@ __device__ bool leaf_window(const SearchCtx &c, PipeNode &s, const uint64_t *sk,
             s.qn += __popc(bal);
         }
         __syncwarp();
-        while (s.qn >= 32) {
-            leaf_drain<LEAF>(sk, s.nl, qb, qm, s.qn, 32u, seed, vload64(node_seed), cb, cm, s.cn);
-            while (s.cn >= 32) rot_drain<LEAF>(cb, cm, s.cn, 32u, vload64(node_seed), node_seed, found);
-        }
-        if (s.cn > 0) rot_drain<LEAF>(cb, cm, s.cn, s.cn, vload64(node_seed), node_seed, found);
+        leaf_phase_bc<LEAF>(sk, s.nl, qb, qm, s.qn, s.keep, s.ckeep, seed, cb, cm, node_seed, found);
+        __syncwarp();  // qb/qm are appended to by the next window
     } else {
         const uint32_t full = (1u << s.m) - 1;
         uint32_t off = 0xFFFFFFFFu;
@@ -526,16 +503,19 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(SearchCtx c, PipeCtx p) {
             s.stage = c.nodes.stage[id];
             s.m = c.nodes.size[id];
             s.budget = budget_for(c, s.m);
-            s.qn = s.cn = 0;
+            s.qn = 0;
             if (s.stage == kStageUpper || s.stage == kStageLower) {
                 const uint32_t start = c.nodes.start[id];
                 for (uint32_t i = lane; i < s.m; i += 32) ask[i] = __ldcg(&c.keys[start + i]);
                 __syncwarp();
                 if (s.stage == kStageUpper) aggr_setup<LEAF, kStageUpper>(c, s);
                 else aggr_setup<LEAF, kStageLower>(c, s);
+                s.keep = search_eagerly(c, s.m, 32u * SA) ? 0 : 31;
             } else {
                 const uint32_t start = c.nodes.start[id];
                 const uint64_t k = lane < (int)s.m ? __ldcg(&c.keys[start + lane]) : 0;
+                s.keep = search_eagerly(c, s.m, (uint64_t)32 * SL * LEAF) ? 0 : 31;
+                s.ckeep = (1ull << (c.tab.memo[s.m] >> 27)) <= (uint64_t)32 * SL * LEAF ? 0 : 31;
                 if (s.stage == kStageLeafRot) {
                     const unsigned even = __ballot_sync(0xffffffffu, lane < (int)s.m && (k & 1) == 0);
                     const unsigned odd = __ballot_sync(0xffffffffu, lane < (int)s.m && (k & 1) == 1);

@@ -22,10 +22,10 @@ namespace {
 // multiply-add per key on a full node (two integer ops more on other nodes; moment_sums and
 // add_part) instead of a packed part count, and that
 // about 1 / (2.5 * sqrt(m * var(p))) of the seeds pass (1.9 % at m = 112, fanout 7).
-// Phase A applies it to every seed of a window (8 or 12 per lane); the survivors go to a per-warp
-// queue in shared memory, and phase B gives each lane one queued seed for the exact part
-// count. A warp drains its queue before it leaves a node, so every seed below the node's
-// final best is still fully checked and the minimum is unchanged.
+// Phase A applies it to every seed of a window (8, 12 or 16 per lane); the survivors go to a
+// per-warp queue in shared memory, and phase B gives each lane one queued seed for the exact
+// part count, lowest seeds first, before the warp takes its next window (aggr_phase_b), so
+// every seed below the node's final best is fully checked and the minimum is unchanged.
 // ---------------------------------------------------------------------------------------
 
 // S = candidates per lane of a window (a stage schedule parameter, StageSchedule): larger
@@ -35,7 +35,7 @@ template <int LEAF, int STAGE, int S_ = 8>
 struct AggrCfg {
     static constexpr int S = S_;
     static constexpr uint32_t W = 32u * S;                  // candidates of one window
-    static constexpr int QCAP = 32 + (int)W;                // < 32 pending after a drain + one window
+    static constexpr int QCAP = 32 + (int)W;                // < 32 carried over + one window's survivors
     static constexpr uint32_t SPLIT = STAGE == kStageUpper ? lower_of(LEAF) : (uint32_t)LEAF;
     static constexpr uint32_t MAXM = STAGE == kStageUpper ? upper_of(LEAF) : lower_of(LEAF);
     static constexpr uint32_t MAXF = (MAXM + SPLIT - 1) / SPLIT;
@@ -75,22 +75,67 @@ __device__ __forceinline__ bool aggr_exact(const uint64_t *sk, uint32_t m, uint3
     return lo == tlo && (!WIDE || hi == thi);
 }
 
-// Phase B: checks the last `take` (<= 32) queued candidates, one per lane, and merges the
-// smallest success into the node's seed. Candidates not below `best` cannot lower it.
+// Phase B: checks the candidates q[0, take) (take <= 32), one per lane, merges the smallest
+// success into the node's seed and returns whether there was one. Candidates not below
+// `best` cannot lower it.
 template <int LEAF, int STAGE>
-__device__ __forceinline__ void aggr_drain(const uint64_t *sk, uint64_t *q, uint32_t &qn, uint32_t take, uint32_t m,
+__device__ __forceinline__ bool aggr_check(const uint64_t *sk, const uint64_t *q, uint32_t take, uint32_t m,
                                            uint32_t fan, bool full, uint64_t seed, uint32_t tlo, uint32_t thi,
                                            uint64_t best, uint64_t *node_seed, uint32_t *found) {
     using C = AggrCfg<LEAF, STAGE>;
     const int lane = threadIdx.x & 31;
     const bool active = lane < (int)take;
-    const uint64_t x = active ? q[qn - take + lane] : ~0ull;
-    __syncwarp();
+    const uint64_t x = active ? q[lane] : ~0ull;
     bool ok = false;
     if (active && x < best) ok = aggr_exact<LEAF, STAGE, C::WIDE>(sk, m, fan, full, seed + x, tlo, thi);
     const uint64_t v = warp_min_u64(ok ? x : ~0ull);
     if (lane == 0 && v != ~0ull) merge_seed(node_seed, v, found);
-    qn -= take;
+    return v != ~0ull;
+}
+
+// Phase B of the queued candidates q[0, qn) (ascending): lowest first, 32 at a time, while more
+// than `keep` are queued, until a batch holds a success (every later candidate is larger) or
+// the node's best is at or below the next candidate; then nothing queued can lower the seed and
+// the queue is emptied. Checked batches leave the queue (the rest moves down).
+//
+// How many a window leaves queued is the node's choice (search_eagerly): a node expected to
+// need few windows checks all of its survivors before its next window (keep = 0), so that its
+// seed is known at once - survivors carried over would let the warp search on past a minimum
+// that sits in its own queue, which at l = 12 doubled the windows per node; a node expected to
+// need hundreds of windows checks full batches only (keep = 31), since a partial batch of a
+// few survivors costs as much as a full one.
+template <int LEAF, int STAGE>
+__device__ __forceinline__ void aggr_phase_b(const uint64_t *sk, uint64_t *q, uint32_t &qn, uint32_t keep, uint32_t m,
+                                             uint32_t fan, bool full, uint64_t seed, uint32_t tlo, uint32_t thi,
+                                             uint64_t *node_seed, uint32_t *found) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t qh = 0;
+    while (qn - qh > keep) {
+        const uint64_t best = warp_load64(node_seed);
+        const uint32_t take = min(qn - qh, 32u);
+        if (q[qh] >= best ||
+            aggr_check<LEAF, STAGE>(sk, q + qh, take, m, fan, full, seed, tlo, thi, best, node_seed, found)) {
+            qn = 0;
+            return;
+        }
+        qh += take;
+    }
+    // the (fewer than 32) unchecked candidates move to the front; qh >= 32 > their count
+    const uint32_t rest = qn - qh;
+    if (qh > 0 && rest > 0) {
+        const uint64_t v = lane < rest ? q[qh + lane] : 0;
+        __syncwarp();
+        if (lane < rest) q[lane] = v;
+        __syncwarp();
+    }
+    qn = rest;
+}
+
+// Whether a node checks every window's survivors before its next window (keep = 0 above): its
+// Golomb-Rice parameter g puts its expected seed near 2^g; `window` is the window's width in
+// the same units (seeds, or encoded seeds b * LEAF + r of rotation leaves).
+__device__ __forceinline__ bool search_eagerly(const SearchCtx &c, uint32_t m, uint64_t window) {
+    return (1ull << (c.tab.memo[m] >> 27)) <= 32ull * window;
 }
 
 template <int LEAF, int STAGE, int S_>
@@ -110,7 +155,7 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
     uint32_t *found = &c.sched[kNumStages + STAGE];  // nodes of this stage with a seed
     const uint64_t seed = start_seed(C::SEED_INDEX);
     uint32_t rng = gw * 2654435761u + 12345u;
-    uint32_t node = kEmpty, m = 0, fan = 0, tlo = 0, thi = 0, t1 = 0, mult = 0, qn = 0;
+    uint32_t node = kEmpty, m = 0, fan = 0, tlo = 0, thi = 0, t1 = 0, mult = 0, qn = 0, keep = 0;
     bool owner = false, full = false;
     uint64_t budget = 0;
     for (;;) {
@@ -150,18 +195,16 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
             for (uint32_t j = 1; j < fan; ++j) t1 += j * (j + 1 < fan ? C::SPLIT : m - (fan - 1) * C::SPLIT);
             budget = budget_for(c, m);
             qn = 0;
+            keep = search_eagerly(c, m, W) ? 0 : 31;
         }
         uint32_t w = 0;
         if (lane == 0) w = atomicAdd(&c.nodes.next_win[node], 1u);
         w = __shfl_sync(0xffffffffu, w, 0);
         const uint64_t x0 = (uint64_t)w * W;
-        uint64_t best = warp_load64(&c.nodes.seed[node]);
+        const uint64_t best = warp_load64(&c.nodes.seed[node]);
         if (x0 >= best || x0 >= budget) {
-            while (qn > 0) {
-                best = vload64(&c.nodes.seed[node]);
-                aggr_drain<LEAF, STAGE>(sk, q, qn, min(qn, 32u), m, fan, full, seed, tlo, thi, best, &c.nodes.seed[node], found);
-            }
-            if (x0 < best && lane == 0) merge_seed(&c.nodes.seed[node], kSeedFailed, found);
+            aggr_phase_b<LEAF, STAGE>(sk, q, qn, 0, m, fan, full, seed, tlo, thi, &c.nodes.seed[node], found);
+            if (x0 < warp_load64(&c.nodes.seed[node]) && lane == 0) merge_seed(&c.nodes.seed[node], kSeedFailed, found);
             if (owner && lane == 0) c.slots[gw] = kEmpty;
             node = kEmpty;
             continue;
@@ -196,10 +239,8 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
             qn += __popc(b);
         }
         __syncwarp();
-        while (qn >= 32) {
-            best = vload64(&c.nodes.seed[node]);
-            aggr_drain<LEAF, STAGE>(sk, q, qn, 32u, m, fan, full, seed, tlo, thi, best, &c.nodes.seed[node], found);
-        }
+        aggr_phase_b<LEAF, STAGE>(sk, q, qn, keep, m, fan, full, seed, tlo, thi, &c.nodes.seed[node], found);
+        __syncwarp();  // q is appended to by the next window
     }
 }
 
@@ -261,7 +302,7 @@ __global__ void __launch_bounds__(kThreads) k_partition_aggr(SearchCtx c) {
 // Brute-force leaves: the first x whose m bit positions are all distinct.
 // ---------------------------------------------------------------------------------------
 // Rotation leaves: S bases per lane of a window (a stage schedule parameter); the queue holds
-// the survivors of one window plus fewer than 32 left over from the last drain.
+// the survivors of one window plus fewer than 32 carried over (leaf_phase_bc).
 template <int S> __host__ __device__ constexpr int leaf_queue_cap() { return 32 + 32 * S; }
 
 template <int LEAF>
@@ -314,20 +355,19 @@ __device__ __forceinline__ void left_masks(const uint64_t *sk, uint32_t nl, uint
     __syncwarp();  // pk is rewritten by the next window
 }
 
-// Phase B of rotation leaves: each lane takes one queued (base, left mask) and computes the
-// base's right mask; the bases whose right keys also land on distinct bits go, with both
-// masks, to the rotation queue (cb, cm) for phase C. Bases not below `best` cannot lower it.
-constexpr uint32_t kRotQueueCap = 64;  // < 32 pending after a phase-C drain + one phase-B drain
+// Phase B of rotation leaves: each lane takes one queued (base, left mask) of qb/qm[0, take)
+// and computes the base's right mask; the bases whose right keys also land on distinct bits
+// go, with both masks, to the rotation queue cb/cm[0, cn) for phase C, in the same order.
+// Bases not below `best` cannot lower it.
+constexpr uint32_t kRotQueueCap = 64;  // < 32 carried over + the phase-B passes of one batch
 
 template <int LEAF>
-__device__ __forceinline__ void leaf_drain(const uint64_t *sk, uint32_t nl, const uint64_t *qb, const uint32_t *qm,
-                                           uint32_t &qn, uint32_t take, uint64_t seed, uint64_t best, uint64_t *cb,
-                                           uint2 *cm, uint32_t &cn) {
+__device__ __forceinline__ uint32_t leaf_check(const uint64_t *sk, uint32_t nl, const uint64_t *qb, const uint32_t *qm,
+                                               uint32_t take, uint64_t seed, uint64_t best, uint64_t *cb, uint2 *cm) {
     const int lane = threadIdx.x & 31;
     const bool active = lane < (int)take;
-    const uint64_t b = active ? qb[qn - take + lane] : 0;
-    const uint32_t ml = active ? qm[qn - take + lane] : 0;
-    __syncwarp();
+    const uint64_t b = active ? qb[lane] : 0;
+    const uint32_t ml = active ? qm[lane] : 0;
     bool pass = false;
     uint32_t mr = 0;
     if (active && b * LEAF < best) {
@@ -337,27 +377,26 @@ __device__ __forceinline__ void leaf_drain(const uint64_t *sk, uint32_t nl, cons
     }
     const unsigned bal = __ballot_sync(0xffffffffu, pass);
     if (pass) {
-        const uint32_t at = cn + __popc(bal & ((1u << lane) - 1));
+        const uint32_t at = __popc(bal & ((1u << lane) - 1));
         cb[at] = b;
         cm[at] = make_uint2(ml, mr);
     }
-    cn += __popc(bal);
-    qn -= take;
     __syncwarp();
+    return __popc(bal);
 }
 
-// Phase C: each lane takes one base whose halves are both collision-free and finds the least
-// left rotation r of the right mask that fills the complement of the left mask; the warp's
-// least b * LEAF + r is merged into the node's seed.
+// Phase C: each lane takes one base of cb/cm[0, cn) whose halves are both collision-free and
+// finds the least left rotation r of the right mask that fills the complement of the left
+// mask; the warp's least b * LEAF + r is merged into the node's seed. Returns whether there
+// was one.
 template <int LEAF>
-__device__ __forceinline__ void rot_drain(const uint64_t *cb, const uint2 *cm, uint32_t &cn, uint32_t take,
-                                          uint64_t best, uint64_t *node_seed, uint32_t *found) {
+__device__ __forceinline__ bool rot_check(const uint64_t *cb, const uint2 *cm, uint32_t cn, uint64_t best,
+                                          uint64_t *node_seed, uint32_t *found) {
     constexpr uint32_t full = (1u << LEAF) - 1;
     const int lane = threadIdx.x & 31;
-    const bool active = lane < (int)take;
-    const uint64_t b = active ? cb[cn - take + lane] : 0;
-    const uint2 mk = active ? cm[cn - take + lane] : make_uint2(0, 0);
-    __syncwarp();
+    const bool active = lane < (int)cn;
+    const uint64_t b = active ? cb[lane] : 0;
+    const uint2 mk = active ? cm[lane] : make_uint2(0, 0);
     uint64_t enc = ~0ull;
     if (active && b * LEAF < best) {
         const uint32_t want = full & ~mk.x;
@@ -370,8 +409,67 @@ __device__ __forceinline__ void rot_drain(const uint64_t *cb, const uint2 *cm, u
     }
     enc = warp_min_u64(enc);
     if (lane == 0 && enc != ~0ull) merge_seed(node_seed, enc, found);
-    cn -= take;
-    __syncwarp();
+    __syncwarp();  // cb/cm are rewritten by the next batch
+    return enc != ~0ull;
+}
+
+// Phases B and C of the queued bases qb/qm[0, qn) (ascending), as aggr_phase_b: phase B takes
+// them lowest first, 32 at a time, while more than `keep` are queued; its passes collect in the
+// rotation queue cb/cm, which phase C checks whenever it holds more than `ckeep` (up to 32 at a
+// time) and, at the end, whatever is left. A phase-C batch with a success ends the checks (every
+// later base is larger, and so is its encoded seed b * LEAF + r), as does a best below the next
+// queued base. ckeep = 0 suits leaves that succeed within a window (each phase-B batch may hold
+// the seed and end the window early), 31 the others (full phase-C batches).
+template <int LEAF>
+__device__ __forceinline__ void leaf_phase_bc(const uint64_t *sk, uint32_t nl, uint64_t *qb, uint32_t *qm, uint32_t &qn,
+                                              uint32_t keep, uint32_t ckeep, uint64_t seed, uint64_t *cb, uint2 *cm,
+                                              uint64_t *node_seed, uint32_t *found) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t qh = 0, cn = 0;
+    bool spent = false;  // every base still queued is at or above the best
+    while (qn - qh > keep) {
+        const uint64_t best = warp_load64(node_seed);
+        if (qb[qh] * LEAF >= best) {
+            spent = true;
+            break;
+        }
+        const uint32_t take = min(qn - qh, 32u);
+        cn += leaf_check<LEAF>(sk, nl, qb + qh, qm + qh, take, seed, best, cb + cn, cm + cn);
+        qh += take;
+        if (cn > ckeep) {
+            const uint32_t ct = min(cn, 32u);
+            if (rot_check<LEAF>(cb, cm, ct, warp_load64(node_seed), node_seed, found)) {
+                qn = 0;
+                return;
+            }
+            cn -= ct;  // the rest (fewer than 32) moves to the front
+            const uint64_t b = lane < cn ? cb[ct + lane] : 0;
+            const uint2 mk = lane < cn ? cm[ct + lane] : make_uint2(0, 0);
+            __syncwarp();
+            if (lane < cn) {
+                cb[lane] = b;
+                cm[lane] = mk;
+            }
+            __syncwarp();
+        }
+    }
+    if (cn > 0 && rot_check<LEAF>(cb, cm, cn, warp_load64(node_seed), node_seed, found)) spent = true;
+    if (spent) {
+        qn = 0;
+        return;
+    }
+    const uint32_t rest = qn - qh;  // fewer than 32 unchecked bases move to the front
+    if (qh > 0 && rest > 0) {
+        const uint64_t b = lane < rest ? qb[qh + lane] : 0;
+        const uint32_t mk = lane < rest ? qm[qh + lane] : 0;
+        __syncwarp();
+        if (lane < rest) {
+            qb[lane] = b;
+            qm[lane] = mk;
+        }
+        __syncwarp();
+    }
+    qn = rest;
 }
 
 // Per-warp shared memory of the leaf search, in bytes: keys and per-key terms (LEAF each),
@@ -395,14 +493,13 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
     uint32_t *qm = reinterpret_cast<uint32_t *>(qb + QCAP);
     uint64_t *cb = reinterpret_cast<uint64_t *>(qm + QCAP);
     uint2 *cm = reinterpret_cast<uint2 *>(cb + kRotQueueCap);
-    uint32_t qn = 0, cn = 0;
     const uint32_t gw = blockIdx.x * kWarpsPerCta + warp;
     const uint32_t count = c.stage_info[STAGE];
     const uint32_t base = c.stage_info[kNumStages + STAGE];
     uint32_t *found = &c.sched[kNumStages + STAGE];  // nodes of this stage with a seed
     const uint64_t seed = start_seed(kNumStartSeeds - 1);
     uint32_t rng = gw * 2654435761u + 777u;
-    uint32_t node = kEmpty, m = 0, nl = 0;
+    uint32_t node = kEmpty, m = 0, nl = 0, qn = 0, keep = 0, ckeep = 0;
     bool owner = false;
     uint64_t budget = 0;
     for (;;) {
@@ -437,25 +534,19 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
             }
             __syncwarp();
             budget = budget_for(c, m);
-            qn = cn = 0;
+            qn = 0;
+            keep = search_eagerly(c, m, (uint64_t)W * LEAF) ? 0 : 31;
+            ckeep = (1ull << (c.tab.memo[m] >> 27)) <= (uint64_t)W * LEAF ? 0 : 31;
         }
         uint32_t w = 0;
         if (lane == 0) w = atomicAdd(&c.nodes.next_win[node], 1u);
         w = __shfl_sync(0xffffffffu, w, 0);
         const uint64_t x0 = (uint64_t)w * W;                   // first base (ROT) or seed of the window
         const uint64_t enc0 = ROT ? x0 * LEAF : x0;            // first encoded seed of the window
-        uint64_t best = warp_load64(&c.nodes.seed[node]);
+        const uint64_t best = warp_load64(&c.nodes.seed[node]);
         if (enc0 >= best || enc0 >= budget) {
-            if (ROT) {
-                while (qn > 0) {
-                    best = vload64(&c.nodes.seed[node]);
-                    leaf_drain<LEAF>(sk, nl, qb, qm, qn, min(qn, 32u), seed, best, cb, cm, cn);
-                    while (cn >= 32) rot_drain<LEAF>(cb, cm, cn, 32u, vload64(&c.nodes.seed[node]), &c.nodes.seed[node], found);
-                }
-                while (cn > 0) rot_drain<LEAF>(cb, cm, cn, min(cn, 32u), vload64(&c.nodes.seed[node]), &c.nodes.seed[node], found);
-                best = vload64(&c.nodes.seed[node]);
-            }
-            if (enc0 < best && lane == 0) merge_seed(&c.nodes.seed[node], kSeedFailed, found);
+            if (ROT) leaf_phase_bc<LEAF>(sk, nl, qb, qm, qn, 0, ckeep, seed, cb, cm, &c.nodes.seed[node], found);
+            if (enc0 < warp_load64(&c.nodes.seed[node]) && lane == 0) merge_seed(&c.nodes.seed[node], kSeedFailed, found);
             if (owner && lane == 0) c.slots[gw] = kEmpty;
             node = kEmpty;
             continue;
@@ -481,14 +572,8 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
                 qn += __popc(bal);
             }
             __syncwarp();
-            while (qn >= 32) {
-                best = vload64(&c.nodes.seed[node]);
-                leaf_drain<LEAF>(sk, nl, qb, qm, qn, 32u, seed, best, cb, cm, cn);
-                while (cn >= 32) rot_drain<LEAF>(cb, cm, cn, 32u, vload64(&c.nodes.seed[node]), &c.nodes.seed[node], found);
-            }
-            // Bases with both halves collision-free are checked within the window that found them,
-            // so that a success is known before the warp takes further windows of the node.
-            if (cn > 0) rot_drain<LEAF>(cb, cm, cn, cn, vload64(&c.nodes.seed[node]), &c.nodes.seed[node], found);
+            leaf_phase_bc<LEAF>(sk, nl, qb, qm, qn, keep, ckeep, seed, cb, cm, &c.nodes.seed[node], found);
+            __syncwarp();  // qb/qm are appended to by the next window
             continue;
         } else {
             const uint32_t full = (1u << m) - 1;
