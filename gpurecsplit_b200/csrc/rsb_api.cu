@@ -212,7 +212,7 @@ rsb_status copy_to_host(rsb_mphf *h, cudaStream_t st) {
 
 // Every search stage in dependency order: fanout-2 depths, then each aggregation level
 // followed by its partition, then the leaves. Records the stage-boundary events.
-uint32_t schedule_key(uint32_t leaf, int stage, int size_class) { return leaf * 256u + (uint32_t)stage * 2u + size_class; }
+uint32_t schedule_key(uint32_t leaf, int stage, int size_class) { return leaf * 256u + (uint32_t)stage * 4u + size_class; }
 
 // The engine's schedule of one stage: a rsb_engine_set_schedule override or the built-in table.
 StageSchedule engine_schedule(const rsb_engine *e, uint32_t leaf, int stage, uint64_t keys) {
@@ -925,7 +925,7 @@ rsb_status rsb_engine_set_pipeline(rsb_engine *e, uint32_t on) {
 
 rsb_status rsb_engine_set_schedule(rsb_engine *e, uint32_t leaf, uint32_t stage, uint32_t size_class,
                                    uint32_t seeds_per_lane, uint32_t occupancy_pct) {
-    if (!e || leaf < 2 || leaf > (uint32_t)kMaxLeafSize || size_class > 1 ||
+    if (!e || leaf < 2 || leaf > (uint32_t)kMaxLeafSize || size_class >= (uint32_t)kScheduleSizeClasses ||
         (stage != (uint32_t)kStageUpper && stage != (uint32_t)kStageLower && stage != (uint32_t)kStageLeafRot))
         return RSB_ERR_BAD_ARG;
     const uint32_t key = schedule_key(leaf, (int)stage, (int)size_class);
@@ -941,7 +941,8 @@ rsb_status rsb_engine_set_schedule(rsb_engine *e, uint32_t leaf, uint32_t stage,
 
 rsb_status rsb_engine_get_schedule(rsb_engine *e, uint32_t leaf, uint32_t stage, uint32_t size_class,
                                    uint32_t *seeds_per_lane, uint32_t *occupancy_pct) {
-    if (!e || !seeds_per_lane || !occupancy_pct || leaf < 2 || leaf > (uint32_t)kMaxLeafSize || size_class > 1 ||
+    if (!e || !seeds_per_lane || !occupancy_pct || leaf < 2 || leaf > (uint32_t)kMaxLeafSize ||
+        size_class >= (uint32_t)kScheduleSizeClasses ||
         (stage != (uint32_t)kStageUpper && stage != (uint32_t)kStageLower && stage != (uint32_t)kStageLeafRot))
         return RSB_ERR_BAD_ARG;
     auto it = e->schedules.find(schedule_key(leaf, (int)stage, (int)size_class));

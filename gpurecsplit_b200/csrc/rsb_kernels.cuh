@@ -87,7 +87,8 @@ struct StageSchedule {
     int seeds_per_lane;
     int occupancy_pct;
 };
-// Size class of a build for the schedule table: 0 below 2^20 keys, 1 from 2^20.
+// Size class of a build for the schedule table: 0 below 2^20 keys, 1 from 2^20, 2 from 2^24.
+constexpr int kScheduleSizeClasses = 3;
 int schedule_size_class(uint64_t keys);
 bool schedule_valid(int stage, const StageSchedule &s);
 // The built-in (tuned) schedule; brute-force leaves always take 8 seeds per lane.

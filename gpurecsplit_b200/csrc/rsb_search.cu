@@ -163,7 +163,7 @@ constexpr ScheduleEntry kTunedSchedules[] = {
 };
 }  // namespace
 
-int schedule_size_class(uint64_t keys) { return keys >= (1ull << 20) ? 1 : 0; }
+int schedule_size_class(uint64_t keys) { return keys >= (1ull << 24) ? 2 : keys >= (1ull << 20) ? 1 : 0; }
 
 bool schedule_valid(int stage, const StageSchedule &s) {
     if (s.occupancy_pct < 1 || s.occupancy_pct > 100) return false;

@@ -7,7 +7,7 @@ Larger windows amortise a window's per-key work over more candidates; smaller on
 a node's minimum seed by less and keep more warps busy at the end of a stage. The best
 choice depends on the leaf size (node sizes, seeds per node) and on the size of the build
 (how long a stage's tail is), so the table is keyed by (leaf size, stage, size class), size
-class 0 below 2^20 keys and 1 from 2^20.
+class 0 below 2^20 keys, 1 from 2^20 and 2 from 2^24 (tuned on 2^17, 2^20 and 2^24 keys).
 
 For each leaf size and size class the tuner builds one synthetic workload (uniform random
 64-bit keys, the bucket size usual for that leaf size) with every candidate schedule - all
@@ -18,7 +18,7 @@ built-in schedule (a schedule never changes the minimum seeds). Results go to
 gpurecsplit_b200/schedules.json (measurements) and gpurecsplit_b200/csrc/rsb_schedules.inc
 (the table compiled into librsb.so as its built-in schedules; rebuild after tuning).
 
-    python -m gpurecsplit_b200.tune [--leaves 4-20] [--repeats 3] [--out DIR]
+    python -m gpurecsplit_b200.tune [--leaves 4-20] [--classes 0,1,2] [--repeats 3] [--out DIR]
 """
 from __future__ import annotations
 
@@ -33,7 +33,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 STAGES = {17: (8, 12, 16), 18: (8, 12, 16), 19: (4, 8, 12)}
 OCCUPANCY = (100, 75)
-CLASS_KEYS = {0: 1 << 17, 1: 1 << 20}
+CLASS_KEYS = {0: 1 << 17, 1: 1 << 20, 2: 1 << 24}
 
 
 def bucket_size_for(leaf: int) -> int:
@@ -135,7 +135,7 @@ def parse_leaves(spec: str) -> list:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--leaves", default="4-20")
-    ap.add_argument("--classes", default="0,1")
+    ap.add_argument("--classes", default="0,1,2")
     ap.add_argument("--repeats", type=int, default=3)
     ap.add_argument("--out", default=HERE, help="directory holding schedules.json and csrc/rsb_schedules.inc")
     ap.add_argument("--log", default=None)
@@ -155,11 +155,13 @@ def main() -> None:
     entries = []
     for leaf in parse_leaves(args.leaves):
         for c in [int(x) for x in args.classes.split(",")]:
-            if c == 1 and leaf > 18:
-                continue  # class-1 builds at l > 18 take minutes each; they use the class-0 result
+            if (c == 1 and leaf > 18) or (c == 2 and leaf > 16):
+                continue  # builds that take minutes each: they use the next smaller class's result
             entries += tune_one(rsb, engine, leaf, c, args.repeats, log)
     for e in [e for e in entries if e["size_class"] == 0 and e["leaf"] > 18]:
         entries.append(dict(e, size_class=1, copied_from_size_class=0))
+    for e in [e for e in entries if e["size_class"] == 1 and e["leaf"] > 16]:
+        entries.append(dict(e, size_class=2, copied_from_size_class=e.get("copied_from_size_class", 1)))
     engine.close()
     write_table(entries, args.out)
 

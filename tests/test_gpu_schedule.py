@@ -41,7 +41,12 @@ def test_schedule_arguments(rsb):
         assert e.schedule(16, 18, 1) == (16, 90)
         e.set_schedule(16, 18, 1, 0)
         assert e.schedule(16, 18, 1) == builtin
-        for args in ((16, 18, 1, 4, 100), (16, 19, 1, 16, 100), (16, 18, 2, 8, 100), (16, 20, 0, 8, 100),
+        e.set_schedule(16, 18, 2, 8, 75)  # size classes are separate entries
+        assert e.schedule(16, 18, 2) == (8, 75) and e.schedule(16, 18, 1) == builtin
+        lower0 = e.schedule(16, 18, 0)
+        e.set_schedule(16, 17, 2, 16, 60)  # the entry of stage 17, class 2 is not stage 18's
+        assert e.schedule(16, 17, 2) == (16, 60) and e.schedule(16, 18, 0) == lower0
+        for args in ((16, 18, 1, 4, 100), (16, 19, 1, 16, 100), (16, 18, 3, 8, 100), (16, 20, 0, 8, 100),
                      (1, 18, 0, 8, 100), (16, 18, 0, 8, 0), (16, 18, 0, 8, 101)):
             with pytest.raises(rsb.RSBError) as err:
                 e.set_schedule(*args)

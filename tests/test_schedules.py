@@ -19,7 +19,7 @@ def _inc_entries():
 def test_table_entries_are_valid():
     seen = set()
     for leaf, stage, cls, s, pct in _inc_entries():
-        assert 2 <= leaf <= 24 and cls in (0, 1) and 1 <= pct <= 100
+        assert 2 <= leaf <= 24 and cls in (0, 1, 2) and 1 <= pct <= 100
         assert s in ((8, 12, 16) if stage in (17, 18) else (4, 8, 12)) and stage in (17, 18, 19)
         assert (leaf, stage, cls) not in seen
         seen.add((leaf, stage, cls))
