@@ -423,8 +423,8 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
             # (one GPU; at N > 1 the line carries the headline only).
             del keys_dev, flush
             torch.cuda.empty_cache()
-            # 1.8 ms per C1 build: 300 timed steps keep the clock sampler (200 ms period) busy
-            line["c1"] = measure_config("c1", engine, steps=300, warmup=3, e2e_steps=2)
+            # 1.2 ms per C1 build: 1000 timed steps keep the clock sampler (200 ms period) busy
+            line["c1"] = measure_config("c1", engine, steps=1000, warmup=3, e2e_steps=2)
             line["c3"] = measure_config("c3", engine, steps=1, warmup=1, e2e_steps=1)
             line["c4_batch"] = measure_batch(args.sets, engine)
             line["c5_serve"] = measure_serve(args.requests, args.max_keys, args.hbm_budget, args.inflight, args.load)
