@@ -217,8 +217,8 @@ __device__ void pipe_complete_aggr(const SearchCtx &c, const PipeCtx &p, uint32_
 
 // Per-node search state of a warp.
 struct PipeNode {
-    uint32_t id, stage, m, fan, tlo, thi, t1, mult, nl, qn, keep, ckeep;
-    bool full, owner;
+    uint32_t id, stage, m, fan, tlo, thi, t1, mult, na, qn, keep, ckeep;
+    bool full, owner, odd_first;
     uint64_t budget;
 };
 
@@ -300,7 +300,7 @@ __device__ bool leaf_window(const SearchCtx &c, PipeNode &s, const uint64_t *sk,
     const uint64_t enc0 = ROT ? x0 * LEAF : x0;
     const uint64_t best = warp_load64(node_seed);
     if (enc0 >= best || enc0 >= s.budget) {
-        if (ROT) leaf_phase_bc<LEAF>(sk, s.nl, qb, qm, s.qn, 0, s.ckeep, seed, cb, cm, node_seed, found);
+        if (ROT) leaf_phase_bc<LEAF>(sk, s.na, s.odd_first, qb, qm, s.qn, 0, s.ckeep, seed, cb, cm, node_seed, found);
         if (enc0 < warp_load64(node_seed) && lane == 0) merge_seed(node_seed, kSeedFailed, found);
         return false;
     }
@@ -309,11 +309,11 @@ __device__ bool leaf_window(const SearchCtx &c, PipeNode &s, const uint64_t *sk,
         uint32_t ml[S];
 #pragma unroll
         for (int k = 0; k < S; ++k) ml[k] = 0;
-        left_masks<LEAF, S>(sk, s.nl, seed + x0 * LEAF, pk, ml);
+        left_masks<LEAF, S>(sk, s.na, seed + x0 * LEAF, pk, ml);
 #pragma unroll
         for (int k = 0; k < S; ++k) {
             const uint64_t b = x0 + lane + 32u * k;
-            const uint32_t mk = left_mask_of<LEAF>(ml[k], s.nl);
+            const uint32_t mk = left_mask_of<LEAF>(ml[k], s.na);
             const bool pass = mk != ~0u;
             const unsigned bal = __ballot_sync(0xffffffffu, pass);
             if (pass) {
@@ -323,7 +323,7 @@ __device__ bool leaf_window(const SearchCtx &c, PipeNode &s, const uint64_t *sk,
             s.qn += __popc(bal);
         }
         __syncwarp();
-        leaf_phase_bc<LEAF>(sk, s.nl, qb, qm, s.qn, s.keep, s.ckeep, seed, cb, cm, node_seed, found);
+        leaf_phase_bc<LEAF>(sk, s.na, s.odd_first, qb, qm, s.qn, s.keep, s.ckeep, seed, cb, cm, node_seed, found);
         __syncwarp();  // qb/qm are appended to by the next window
     } else {
         const uint32_t full = (1u << s.m) - 1;
@@ -516,12 +516,15 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(SearchCtx c, PipeCtx p) {
                 const uint64_t k = lane < (int)s.m ? __ldcg(&c.keys[start + lane]) : 0;
                 s.keep = search_eagerly(c, s.m, (uint64_t)32 * SL * LEAF) ? 0 : 31;
                 s.ckeep = (1ull << (c.tab.memo[s.m] >> 27)) <= (uint64_t)32 * SL * LEAF ? 0 : 31;
-                if (s.stage == kStageLeafRot) {
+                if (s.stage == kStageLeafRot) {  // phase-A half first, as in k_search_leaf
                     const unsigned even = __ballot_sync(0xffffffffu, lane < (int)s.m && (k & 1) == 0);
                     const unsigned odd = __ballot_sync(0xffffffffu, lane < (int)s.m && (k & 1) == 1);
-                    s.nl = __popc(even);
+                    s.odd_first = __popc(odd) > __popc(even);
+                    const unsigned first = s.odd_first ? odd : even, second = s.odd_first ? even : odd;
+                    s.na = __popc(first);
                     const unsigned below = (1u << lane) - 1;
-                    if (lane < (int)s.m) lsk[(k & 1) ? s.nl + __popc(odd & below) : __popc(even & below)] = k;
+                    const bool in_first = lane < (int)s.m && ((k & 1) != 0) == s.odd_first;
+                    if (lane < (int)s.m) lsk[in_first ? __popc(first & below) : s.na + __popc(second & below)] = k;
                 } else if (lane < (int)s.m) {
                     lsk[lane] = k;
                 }

@@ -296,9 +296,12 @@ __global__ void __launch_bounds__(kThreads) k_partition_aggr(SearchCtx c) {
 // ---------------------------------------------------------------------------------------
 // Leaves. Rotation leaves (m == LEAF): left = even `second`, right = odd; for base b the
 // encoded seed is b*LEAF + r with r the least left rotation of the right mask that fills
-// the complement of the left mask. A base can only succeed if the left keys land on
-// distinct bits, so phase A computes the left mask of every base and queues (base, mask)
-// for the few collision-free ones; phase B computes their right masks and rotations.
+// the complement of the left mask. A base can only succeed if both halves land on distinct
+// bits, so phase A computes the mask of one half for every base and queues (base, mask) for
+// the collision-free ones; phase B computes the other half's mask of those, phase C the
+// rotation. Phase A takes the larger half (the odd keys when there are more of them): its
+// keys collide more often, so fewer bases reach the per-base work of phase B - for a leaf
+// of 3 even and 9 odd keys at l = 12, 1.5 % of the bases instead of 76 %.
 // Brute-force leaves: the first x whose m bit positions are all distinct.
 // ---------------------------------------------------------------------------------------
 // Rotation leaves: S bases per lane of a window (a stage schedule parameter); the queue holds
@@ -311,8 +314,8 @@ __device__ __forceinline__ uint32_t rotl_leaf(uint32_t v, uint32_t r) {
     return ((v << r) | (v >> (LEAF - r))) & full;
 }
 
-// Left-mask sums (add_bit) of the S bases x0 + lane + 32 s of a rotation-leaf window
-// (bu = SEED + x0*LEAF) over the nl < 32 left keys sk[0, nl), with moment_sums' per-key terms:
+// Mask sums (add_bit) of the S bases x0 + lane + 32 s of a rotation-leaf window
+// (bu = SEED + x0*LEAF) over the nl phase-A keys sk[0, nl), with moment_sums' per-key terms:
 // the window spans 32*S*LEAF seeds, each key's (K', L) goes to pk[0, nf) and the indexes of
 // keys whose low half can overflow within the window to pk[LEAF - ns, LEAF).
 template <int LEAF, int S>
@@ -361,9 +364,12 @@ __device__ __forceinline__ void left_masks(const uint64_t *sk, uint32_t nl, uint
 // Bases not below `best` cannot lower it.
 constexpr uint32_t kRotQueueCap = 64;  // < 32 carried over + the phase-B passes of one batch
 
+// The keys are ordered phase-A half first (na keys) and `odd_first` says which half that is;
+// the rotation queue holds (left mask, right mask) whichever half came first.
 template <int LEAF>
-__device__ __forceinline__ uint32_t leaf_check(const uint64_t *sk, uint32_t nl, const uint64_t *qb, const uint32_t *qm,
-                                               uint32_t take, uint64_t seed, uint64_t best, uint64_t *cb, uint2 *cm) {
+__device__ __forceinline__ uint32_t leaf_check(const uint64_t *sk, uint32_t na, bool odd_first, const uint64_t *qb,
+                                               const uint32_t *qm, uint32_t take, uint64_t seed, uint64_t best,
+                                               uint64_t *cb, uint2 *cm) {
     const int lane = threadIdx.x & 31;
     const bool active = lane < (int)take;
     const uint64_t b = active ? qb[lane] : 0;
@@ -372,14 +378,14 @@ __device__ __forceinline__ uint32_t leaf_check(const uint64_t *sk, uint32_t nl, 
     uint32_t mr = 0;
     if (active && b * LEAF < best) {
         const uint64_t bx = seed + b * LEAF;
-        for (uint32_t i = nl; i < (uint32_t)LEAF; ++i) mr |= 1u << remap16(sk[i] + bx, LEAF);
-        pass = __popc(mr) == LEAF - (int)nl;
+        for (uint32_t i = na; i < (uint32_t)LEAF; ++i) mr |= 1u << remap16(sk[i] + bx, LEAF);
+        pass = __popc(mr) == LEAF - (int)na;
     }
     const unsigned bal = __ballot_sync(0xffffffffu, pass);
     if (pass) {
         const uint32_t at = __popc(bal & ((1u << lane) - 1));
         cb[at] = b;
-        cm[at] = make_uint2(ml, mr);
+        cm[at] = odd_first ? make_uint2(mr, ml) : make_uint2(ml, mr);
     }
     __syncwarp();
     return __popc(bal);
@@ -421,7 +427,8 @@ __device__ __forceinline__ bool rot_check(const uint64_t *cb, const uint2 *cm, u
 // queued base. ckeep = 0 suits leaves that succeed within a window (each phase-B batch may hold
 // the seed and end the window early), 31 the others (full phase-C batches).
 template <int LEAF>
-__device__ __forceinline__ void leaf_phase_bc(const uint64_t *sk, uint32_t nl, uint64_t *qb, uint32_t *qm, uint32_t &qn,
+__device__ __forceinline__ void leaf_phase_bc(const uint64_t *sk, uint32_t na, bool odd_first, uint64_t *qb,
+                                              uint32_t *qm, uint32_t &qn,
                                               uint32_t keep, uint32_t ckeep, uint64_t seed, uint64_t *cb, uint2 *cm,
                                               uint64_t *node_seed, uint32_t *found) {
     const uint32_t lane = threadIdx.x & 31;
@@ -434,7 +441,7 @@ __device__ __forceinline__ void leaf_phase_bc(const uint64_t *sk, uint32_t nl, u
             break;
         }
         const uint32_t take = min(qn - qh, 32u);
-        cn += leaf_check<LEAF>(sk, nl, qb + qh, qm + qh, take, seed, best, cb + cn, cm + cn);
+        cn += leaf_check<LEAF>(sk, na, odd_first, qb + qh, qm + qh, take, seed, best, cb + cn, cm + cn);
         qh += take;
         if (cn > ckeep) {
             const uint32_t ct = min(cn, 32u);
@@ -499,8 +506,8 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
     uint32_t *found = &c.sched[kNumStages + STAGE];  // nodes of this stage with a seed
     const uint64_t seed = start_seed(kNumStartSeeds - 1);
     uint32_t rng = gw * 2654435761u + 777u;
-    uint32_t node = kEmpty, m = 0, nl = 0, qn = 0, keep = 0, ckeep = 0;
-    bool owner = false;
+    uint32_t node = kEmpty, m = 0, na = 0, qn = 0, keep = 0, ckeep = 0;
+    bool owner = false, odd_first = false;
     uint64_t budget = 0;
     for (;;) {
         if (node == kEmpty) {
@@ -524,11 +531,15 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
             const uint64_t k = lane < (int)m ? c.keys[start + lane] : 0;
             __syncwarp();
             if (ROT) {
+                // phase-A half first: the larger one (see leaf_check)
                 const unsigned even = __ballot_sync(0xffffffffu, lane < (int)m && (k & 1) == 0);
                 const unsigned odd = __ballot_sync(0xffffffffu, lane < (int)m && (k & 1) == 1);
-                nl = __popc(even);
+                odd_first = __popc(odd) > __popc(even);
+                const unsigned first = odd_first ? odd : even, second = odd_first ? even : odd;
+                na = __popc(first);
                 const unsigned below = (1u << lane) - 1;
-                if (lane < (int)m) sk[(k & 1) ? nl + __popc(odd & below) : __popc(even & below)] = k;
+                const bool in_first = lane < (int)m && ((k & 1) != 0) == odd_first;
+                if (lane < (int)m) sk[in_first ? __popc(first & below) : na + __popc(second & below)] = k;
             } else {
                 if (lane < (int)m) sk[lane] = k;
             }
@@ -545,7 +556,7 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
         const uint64_t enc0 = ROT ? x0 * LEAF : x0;            // first encoded seed of the window
         const uint64_t best = warp_load64(&c.nodes.seed[node]);
         if (enc0 >= best || enc0 >= budget) {
-            if (ROT) leaf_phase_bc<LEAF>(sk, nl, qb, qm, qn, 0, ckeep, seed, cb, cm, &c.nodes.seed[node], found);
+            if (ROT) leaf_phase_bc<LEAF>(sk, na, odd_first, qb, qm, qn, 0, ckeep, seed, cb, cm, &c.nodes.seed[node], found);
             if (enc0 < warp_load64(&c.nodes.seed[node]) && lane == 0) merge_seed(&c.nodes.seed[node], kSeedFailed, found);
             if (owner && lane == 0) c.slots[gw] = kEmpty;
             node = kEmpty;
@@ -558,11 +569,11 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
             uint32_t ml[S];
 #pragma unroll
             for (int s = 0; s < S; ++s) ml[s] = 0;
-            left_masks<LEAF, S>(sk, nl, seed + x0 * LEAF, pk, ml);
+            left_masks<LEAF, S>(sk, na, seed + x0 * LEAF, pk, ml);
 #pragma unroll
             for (int s = 0; s < S; ++s) {
                 const uint64_t b = x0 + lane + 32u * s;
-                const uint32_t mk = left_mask_of<LEAF>(ml[s], nl);
+                const uint32_t mk = left_mask_of<LEAF>(ml[s], na);
                 const bool pass = mk != ~0u;
                 const unsigned bal = __ballot_sync(0xffffffffu, pass);
                 if (pass) {
@@ -572,7 +583,7 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
                 qn += __popc(bal);
             }
             __syncwarp();
-            leaf_phase_bc<LEAF>(sk, nl, qb, qm, qn, keep, ckeep, seed, cb, cm, &c.nodes.seed[node], found);
+            leaf_phase_bc<LEAF>(sk, na, odd_first, qb, qm, qn, keep, ckeep, seed, cb, cm, &c.nodes.seed[node], found);
             __syncwarp();  // qb/qm are appended to by the next window
             continue;
         } else {
