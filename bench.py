@@ -890,12 +890,13 @@ def measure_pipeline(reps: int = 3) -> dict:
     return {"mode": "pipeline", "unit": "ms", "workloads": rows}
 
 
-def measure_builds(n: int, leaf: int, bucket: int, builds: int) -> dict:
-    """`builds` plain builds of n splitmix64 u64 keys (seed 42) on one engine, for profiling
-    the search kernels on a chosen size: the per-stage evaluations, times and windows of the
-    last build."""
+def measure_builds(n: int, leaf: int, bucket: int, builds: int, pipeline: bool = False) -> dict:
+    """`builds` plain builds of n splitmix64 u64 keys (seed 42) on one engine (in pipeline mode
+    with `pipeline`), for profiling the search kernels on a chosen size: the per-stage
+    evaluations, times and windows of the last build."""
     import gpurecsplit_b200 as rsb
     e = rsb.Engine(0)
+    e.set_pipeline(pipeline)
     keys = splitmix64_keys(42, n)
     st = None
     for _ in range(builds):
@@ -905,7 +906,8 @@ def measure_builds(n: int, leaf: int, bucket: int, builds: int) -> dict:
     e.close()
     stages = {s: {"evals": int(st["evals_stage"][s]), "ms": round(st["ms_search"][s], 3),
                   "windows": int(st["windows_stage"][s])} for s in range(17, 21)}
-    return {"mode": "build", "n": n, "leaf": leaf, "bucket": bucket, "builds": builds, "stages": stages}
+    return {"mode": "build", "n": n, "leaf": leaf, "bucket": bucket, "builds": builds, "pipeline": pipeline,
+            "stages": stages}
 
 
 def main() -> None:
@@ -922,6 +924,7 @@ def main() -> None:
     ap.add_argument("--leaf", type=int, default=16, help="--mode build: leaf size")
     ap.add_argument("--bucket", type=int, default=2000, help="--mode build: bucket size")
     ap.add_argument("--builds", type=int, default=2, help="--mode build: builds on one engine")
+    ap.add_argument("--pipeline", action="store_true", help="--mode build: in pipeline mode")
     ap.add_argument("--requests", type=int, default=100)
     ap.add_argument("--max-keys", type=int, default=10_000_000)
     ap.add_argument("--hbm-budget", type=int, default=32 << 30)
@@ -933,7 +936,7 @@ def main() -> None:
         print(json.dumps(measure_batch(args.sets)), flush=True)
         return
     if args.mode == "build":
-        print(json.dumps(measure_builds(args.n, args.leaf, args.bucket, args.builds)), flush=True)
+        print(json.dumps(measure_builds(args.n, args.leaf, args.bucket, args.builds, args.pipeline)), flush=True)
         return
     if args.mode == "pipeline":
         print(json.dumps(measure_pipeline()), flush=True)

@@ -612,12 +612,12 @@ namespace search_impl {
 template <typename K>
 void launch_persistent(K k, const SearchCtx &c, size_t smem, const StageSchedule &s, cudaStream_t st) {
     if (smem) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    use_max_smem(k);  // before the occupancy query, which follows the kernel's carveout preference
     const int pct = std::max(1, c.occupancy_pct * s.occupancy_pct / 100);
     int g = persistent_grid(k, smem, c.num_sms, kThreads, pct);
     g = min(g, (int)(c.nslots / kWarpsPerCta));
     SearchCtx cc = c;
     cc.nslots = g * kWarpsPerCta;
-    use_max_smem(k);
     k<<<g, kThreads, smem, st>>>(cc);
 }
 
@@ -626,12 +626,12 @@ template <typename K>
 void launch_persistent_with(K k, const SearchCtx &c, const PipeCtx &p, size_t smem, const StageSchedule &s,
                             cudaStream_t st) {
     if (smem) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    use_max_smem(k);  // before the occupancy query, which follows the kernel's carveout preference
     const int pct = std::max(1, c.occupancy_pct * s.occupancy_pct / 100);
     int g = persistent_grid(k, smem, c.num_sms, kThreads, pct);
     g = min(g, (int)(c.nslots / kWarpsPerCta));
     SearchCtx cc = c;
     cc.nslots = g * kWarpsPerCta;
-    use_max_smem(k);
     k<<<g, kThreads, smem, st>>>(cc, p);
 }
 
