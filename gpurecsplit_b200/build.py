@@ -20,8 +20,10 @@ LIB = os.path.join(LIB_DIR, "librsb.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# Diagnostic 940 (a non-void function that can end without a return) is an error: its value
+# would be undefined on the device.
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fno-fast-math",
-              "--fmad=false", "-I", INCLUDE]
+              "--fmad=false", "--diag-error", "940", "-I", INCLUDE]
 
 
 def _nvcc() -> str:

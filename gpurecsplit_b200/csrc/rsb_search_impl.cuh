@@ -104,8 +104,12 @@ __device__ __forceinline__ bool aggr_check(const uint64_t *sk, const uint64_t *q
 // that sits in its own queue, which at l = 12 doubled the windows per node; a node expected to
 // need hundreds of windows checks full batches only (keep = 31), since a partial batch of a
 // few survivors costs as much as a full one.
+//
+// Returns true when the node's seed is known to lie below the next window (a success here, or
+// a best at or below a queued candidate): the warp can leave the node without taking another
+// window.
 template <int LEAF, int STAGE>
-__device__ __forceinline__ void aggr_phase_b(const uint64_t *sk, uint64_t *q, uint32_t &qn, uint32_t keep, uint32_t m,
+__device__ __forceinline__ bool aggr_phase_b(const uint64_t *sk, uint64_t *q, uint32_t &qn, uint32_t keep, uint32_t m,
                                              uint32_t fan, bool full, uint64_t seed, uint32_t tlo, uint32_t thi,
                                              uint64_t *node_seed, uint32_t *found) {
     const uint32_t lane = threadIdx.x & 31;
@@ -116,7 +120,7 @@ __device__ __forceinline__ void aggr_phase_b(const uint64_t *sk, uint64_t *q, ui
         if (q[qh] >= best ||
             aggr_check<LEAF, STAGE>(sk, q + qh, take, m, fan, full, seed, tlo, thi, best, node_seed, found)) {
             qn = 0;
-            return;
+            return true;
         }
         qh += take;
     }
@@ -129,6 +133,7 @@ __device__ __forceinline__ void aggr_phase_b(const uint64_t *sk, uint64_t *q, ui
         __syncwarp();
     }
     qn = rest;
+    return false;
 }
 
 // Whether a node checks every window's survivors before its next window (keep = 0 above): its
@@ -239,8 +244,13 @@ __global__ void __launch_bounds__(kThreads) k_search_aggr(SearchCtx c) {
             qn += __popc(b);
         }
         __syncwarp();
-        aggr_phase_b<LEAF, STAGE>(sk, q, qn, keep, m, fan, full, seed, tlo, thi, &c.nodes.seed[node], found);
+        const bool done = aggr_phase_b<LEAF, STAGE>(sk, q, qn, keep, m, fan, full, seed, tlo, thi,
+                                                    &c.nodes.seed[node], found);
         __syncwarp();  // q is appended to by the next window
+        if (done) {  // every later window starts above the node's seed: leave without taking one
+            if (owner && lane == 0) c.slots[gw] = kEmpty;
+            node = kEmpty;
+        }
     }
 }
 
@@ -425,9 +435,10 @@ __device__ __forceinline__ bool rot_check(const uint64_t *cb, const uint2 *cm, u
 // time) and, at the end, whatever is left. A phase-C batch with a success ends the checks (every
 // later base is larger, and so is its encoded seed b * LEAF + r), as does a best below the next
 // queued base. ckeep = 0 suits leaves that succeed within a window (each phase-B batch may hold
-// the seed and end the window early), 31 the others (full phase-C batches).
+// the seed and end the window early), 31 the others (full phase-C batches). Returns true when
+// the leaf's seed is known to lie below the next window, as aggr_phase_b.
 template <int LEAF>
-__device__ __forceinline__ void leaf_phase_bc(const uint64_t *sk, uint32_t na, bool odd_first, uint64_t *qb,
+__device__ __forceinline__ bool leaf_phase_bc(const uint64_t *sk, uint32_t na, bool odd_first, uint64_t *qb,
                                               uint32_t *qm, uint32_t &qn,
                                               uint32_t keep, uint32_t ckeep, uint64_t seed, uint64_t *cb, uint2 *cm,
                                               uint64_t *node_seed, uint32_t *found) {
@@ -447,7 +458,7 @@ __device__ __forceinline__ void leaf_phase_bc(const uint64_t *sk, uint32_t na, b
             const uint32_t ct = min(cn, 32u);
             if (rot_check<LEAF>(cb, cm, ct, warp_load64(node_seed), node_seed, found)) {
                 qn = 0;
-                return;
+                return true;
             }
             cn -= ct;  // the rest (fewer than 32) moves to the front
             const uint64_t b = lane < cn ? cb[ct + lane] : 0;
@@ -463,7 +474,7 @@ __device__ __forceinline__ void leaf_phase_bc(const uint64_t *sk, uint32_t na, b
     if (cn > 0 && rot_check<LEAF>(cb, cm, cn, warp_load64(node_seed), node_seed, found)) spent = true;
     if (spent) {
         qn = 0;
-        return;
+        return true;
     }
     const uint32_t rest = qn - qh;  // fewer than 32 unchecked bases move to the front
     if (qh > 0 && rest > 0) {
@@ -477,6 +488,7 @@ __device__ __forceinline__ void leaf_phase_bc(const uint64_t *sk, uint32_t na, b
         __syncwarp();
     }
     qn = rest;
+    return false;
 }
 
 // Per-warp shared memory of the leaf search, in bytes: keys and per-key terms (LEAF each),
@@ -583,8 +595,13 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
                 qn += __popc(bal);
             }
             __syncwarp();
-            leaf_phase_bc<LEAF>(sk, na, odd_first, qb, qm, qn, keep, ckeep, seed, cb, cm, &c.nodes.seed[node], found);
+            const bool done =
+                leaf_phase_bc<LEAF>(sk, na, odd_first, qb, qm, qn, keep, ckeep, seed, cb, cm, &c.nodes.seed[node], found);
             __syncwarp();  // qb/qm are appended to by the next window
+            if (done) {  // as in k_search_aggr
+                if (owner && lane == 0) c.slots[gw] = kEmpty;
+                node = kEmpty;
+            }
             continue;
         } else {
             const uint32_t full = (1u << m) - 1;
@@ -597,8 +614,13 @@ __global__ void __launch_bounds__(kThreads) k_search_leaf(SearchCtx c) {
             }
         }
         off = __reduce_min_sync(0xffffffffu, off);
-        if (off != 0xFFFFFFFFu && lane == 0)
-            merge_seed(&c.nodes.seed[node], enc0 + off, found);
+        if (off != 0xFFFFFFFFu) {  // this window holds the seed: leave without taking another one
+            if (lane == 0) {
+                merge_seed(&c.nodes.seed[node], enc0 + off, found);
+                if (owner) c.slots[gw] = kEmpty;
+            }
+            node = kEmpty;
+        }
     }
 }
 
