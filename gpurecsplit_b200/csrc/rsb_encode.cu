@@ -220,20 +220,55 @@ __global__ void k_ef_fill(const uint64_t *cum, const uint64_t *pos, uint64_t nb,
 
 // Algorithmic work of the searches: sum over nodes of (candidates up to the found seed) * m,
 // candidates being seeds (splits, brute-force leaves) or rotation bases (rotation leaves).
+// Nodes of the four search stages (almost all nodes) sum in registers and then per warp, so
+// that a block's threads do not all contend for the same few shared-memory counters; the
+// fanout-2 stages add to shared memory directly.
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 __global__ void k_evals(const uint64_t *node_total, NodeArrays nodes, uint32_t leaf, uint32_t rotate, EfParams *ef,
                         uint64_t *windows) {
+    constexpr int kSearch = kNumStages - kStageUpper;  // stages kStageUpper .. kNumStages - 1
     __shared__ unsigned long long s_acc[kNumStages], s_win[kNumStages];
     for (int s = threadIdx.x; s < kNumStages; s += blockDim.x) s_acc[s] = s_win[s] = 0;
     __syncthreads();
+    unsigned long long acc[kSearch], win[kSearch];
+#pragma unroll
+    for (int k = 0; k < kSearch; ++k) acc[k] = win[k] = 0;
     const uint64_t n = *node_total;
     for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t x = nodes.seed[j];
         const uint32_t m = nodes.size[j];
         const uint32_t stage = nodes.stage[j];
-        if (stage >= kStageUpper) atomicAdd(&s_win[stage], (unsigned long long)nodes.next_win[j]);
-        if (x >= kSeedFailed) continue;
+        const bool ok = x < kSeedFailed;
         const uint64_t trials = (rotate && m == leaf) ? x / leaf + 1 : x + 1;
-        atomicAdd(&s_acc[stage], (unsigned long long)(trials * m));
+        const unsigned long long work = ok ? (unsigned long long)(trials * m) : 0ull;
+        if (stage >= (uint32_t)kStageUpper) {
+            const unsigned long long w = nodes.next_win[j];
+#pragma unroll
+            for (int k = 0; k < kSearch; ++k)
+                if (stage == (uint32_t)(kStageUpper + k)) {
+                    acc[k] += work;
+                    win[k] += w;
+                }
+        } else if (ok) {
+            atomicAdd(&s_acc[stage], work);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < kSearch; ++k) {
+        acc[k] = warp_sum_u64(acc[k]);
+        win[k] = warp_sum_u64(win[k]);
+    }
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int k = 0; k < kSearch; ++k) {
+            if (acc[k]) atomicAdd(&s_acc[kStageUpper + k], acc[k]);
+            if (win[k]) atomicAdd(&s_win[kStageUpper + k], win[k]);
+        }
     }
     __syncthreads();
     for (int s = threadIdx.x; s < kNumStages; s += blockDim.x) {

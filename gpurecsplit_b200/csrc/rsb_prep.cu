@@ -146,14 +146,51 @@ __global__ void k_hash_u64(const uint64_t *__restrict__ keys, uint64_t n, ulongl
     }
 }
 
-// Key i is bytes[offsets[i] - base, offsets[i + 1] - base).
-__global__ void k_hash_strings(const uint8_t *__restrict__ bytes, const uint64_t *__restrict__ offsets, uint64_t n,
-                               uint64_t base, ulonglong2 *__restrict__ out) {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t b = offsets[i], e = offsets[i + 1];
+// Key i is bytes[offsets[i] - base, offsets[i + 1] - base). Each warp takes 32 consecutive
+// keys, whose bytes are contiguous: it copies them into shared memory with coalesced 16-byte
+// loads (the unaligned head and tail byte by byte, so that no load leaves the warp's own
+// bytes), then each lane hashes its key from there through aligned 32-bit reads (byte reads
+// of the warp's keys at scattered offsets cost a shared-memory wavefront per byte). A warp
+// whose bytes exceed its buffer, or whose offsets are not non-decreasing, hashes from global
+// memory, one key per lane.
+constexpr int kHashThreads = 128;
+constexpr uint32_t kHashWarpBytes = 2048;  // staged bytes per warp, from the 16-byte block of the first
+
+__global__ void __launch_bounds__(kHashThreads) k_hash_strings(const uint8_t *__restrict__ bytes,
+                                                               const uint64_t *__restrict__ offsets, uint64_t n,
+                                                               uint64_t base, ulonglong2 *__restrict__ out) {
+    __shared__ __align__(16) uint8_t staged[kHashThreads / 32][kHashWarpBytes];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint8_t *buf = staged[warp];
+    const uint64_t stride = (uint64_t)gridDim.x * kHashThreads;
+    for (uint64_t i0 = blockIdx.x * (uint64_t)kHashThreads + warp * 32u; i0 < n; i0 += stride) {
+        const uint64_t i = i0 + lane;
+        const bool valid = i < n;
+        const uint64_t iend = n - i0 < 32 ? n : i0 + 32;
+        const uint64_t gb = offsets[i0], ge = offsets[iend];  // the warp's bytes, before rebasing
+        const uint64_t b = valid ? offsets[i] : gb, e = valid ? offsets[i + 1] : gb;
+        const uintptr_t a0 = (uintptr_t)(bytes + (gb - base)), a1 = (uintptr_t)(bytes + (ge - base));
+        const uintptr_t al0 = a0 & ~(uintptr_t)15;
+        const bool inside = gb <= b && b <= e && e <= ge;
+        const bool stage = __all_sync(0xffffffffu, inside) && gb <= ge && a1 - al0 <= kHashWarpBytes;
         uint64_t h0 = 0, h1 = 0;
-        spooky128(bytes + (b - base), e - b, h0, h1);
-        out[i] = make_ulonglong2(h1, h0);  // first = h1, second = h0 (util/Hash128.h:35)
+        if (stage) {
+            const uintptr_t m0 = (a0 + 15) & ~(uintptr_t)15, m1 = a1 & ~(uintptr_t)15;
+            if (m0 < m1) {
+                for (uintptr_t a = a0 + lane; a < m0; a += 32) buf[a - al0] = *(const uint8_t *)a;
+                for (uintptr_t a = m0 + 16u * lane; a < m1; a += 16u * 32)
+                    *(uint4 *)(buf + (a - al0)) = *(const uint4 *)a;
+                for (uintptr_t a = m1 + lane; a < a1; a += 32) buf[a - al0] = *(const uint8_t *)a;
+            } else {
+                for (uintptr_t a = a0 + lane; a < a1; a += 32) buf[a - al0] = *(const uint8_t *)a;
+            }
+            __syncwarp();
+            if (valid) spooky128<true>(buf + (a0 - al0) + (b - gb), e - b, h0, h1);  // word reads
+            __syncwarp();  // buf is rewritten by the next 32 keys
+        } else if (valid) {
+            spooky128(bytes + (b - base), e - b, h0, h1);
+        }
+        if (valid) out[i] = make_ulonglong2(h1, h0);  // first = h1, second = h0 (util/Hash128.h:35)
     }
 }
 
@@ -185,22 +222,69 @@ __global__ void k_bucket_check(const uint32_t *counts, uint64_t nb, DevStatus *s
 
 // Duplicate check: two keys with the same second half in one bucket always collide, so the
 // reference's search would never end (GPURecSplit.cuh:436); here the build fails with
-// RSB_ERR_DUPLICATE_KEY. Each CTA inserts a bucket's second halves into an open-addressing
-// table in shared memory (read-only pass over the keys). The key order inside a bucket is
+// RSB_ERR_DUPLICATE_KEY. A warp (buckets of at most 256 keys) or a CTA (larger buckets)
+// inserts a bucket's second halves into an open-addressing table in shared memory (read-only
+// pass over the keys); a second key equal to the empty-slot marker is counted instead. The
+// key order inside a bucket is
 // left as the scatter produced it: every seed depends only on the set of a node's keys.
 constexpr int kSortThreads = 256;
 constexpr int kSortCap = 4096;  // > 2 * (kMaxBucketSize - 1) / 1.5: table at most 3/4 full
 constexpr uint64_t kEmptyKey = ~0ull;
 static_assert(4 * (kMaxBucketSize - 1) <= 3 * kSortCap, "duplicate table too small");
 
+constexpr uint32_t kWarpDupMax = 256;                           // buckets up to this size: one warp each
+constexpr uint32_t kWarpDupSlots = kSortCap / (kSortThreads / 32);  // a warp's slice of the table
+static_assert(2 * kWarpDupMax <= kWarpDupSlots, "warp table too small");
+
+// Inserts k into the open-addressing table tab[0, size); returns whether it was there.
+__device__ __forceinline__ bool dup_insert(uint64_t *tab, uint32_t size, uint64_t k) {
+    // `second` is a hash output, so its low bits are a uniform slot; linear probing visits at
+    // most `size` slots and the table is at most 3/4 full.
+    uint32_t slot = (uint32_t)k & (size - 1);
+    for (uint32_t probe = 0; probe < size; ++probe) {
+        const uint64_t prev = atomicCAS((unsigned long long *)&tab[slot], kEmptyKey, k);
+        if (prev == kEmptyKey) return false;
+        if (prev == k) return true;
+        slot = (slot + 1) & (size - 1);
+    }
+    return false;
+}
+
 __global__ void __launch_bounds__(kSortThreads) k_bucket_dupcheck(const uint64_t *sorted, const uint64_t *acc,
                                                                   uint64_t nb, DevStatus *status) {
     __shared__ uint64_t tab[kSortCap];
     __shared__ uint32_t n_empty_key;  // keys equal to the empty-slot marker
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // Buckets of at most kWarpDupMax keys: one warp each, in its own slice of the table, so
+    // the warps of a CTA check different buckets at once.
+    uint64_t *wt = tab + warp * kWarpDupSlots;
+    const uint64_t nw = (uint64_t)gridDim.x * (kSortThreads / 32);
+    for (uint64_t b = blockIdx.x * (uint64_t)(kSortThreads / 32) + warp; b < nb; b += nw) {
+        const uint64_t off = acc[b];
+        const uint32_t m = (uint32_t)(acc[b + 1] - off);
+        if (m <= 1 || m > kWarpDupMax) continue;
+        uint32_t size = 64;
+        while (size < 2 * m) size <<= 1;
+        for (uint32_t i = lane; i < size; i += 32) wt[i] = kEmptyKey;
+        __syncwarp();
+        bool dup = false;
+        uint32_t empties = 0;
+        for (uint32_t i = lane; i < m; i += 32) {
+            const uint64_t k = sorted[off + i];
+            if (k == kEmptyKey) ++empties;
+            else dup |= dup_insert(wt, size, k);
+        }
+        empties = __reduce_add_sync(0xffffffffu, empties);
+        if (__any_sync(0xffffffffu, dup) || empties > 1) {
+            if (lane == 0) set_error(status, RSB_ERR_DUPLICATE_KEY, b);
+        }
+        __syncwarp();  // the slice is cleared for the warp's next bucket
+    }
+    __syncthreads();  // the whole table serves the larger buckets below
     for (uint64_t b = blockIdx.x; b < nb; b += gridDim.x) {
         const uint64_t off = acc[b];
         const uint32_t m = (uint32_t)(acc[b + 1] - off);
-        if (m <= 1 || m > (uint32_t)kMaxBucketSize) continue;  // oversize buckets: k_bucket_check
+        if (m <= kWarpDupMax || m > (uint32_t)kMaxBucketSize) continue;  // oversize buckets: k_bucket_check
         uint32_t size = 64;
         while (size < 2 * m && size < (uint32_t)kSortCap) size <<= 1;
         for (uint32_t i = threadIdx.x; i < size; i += kSortThreads) tab[i] = kEmptyKey;
@@ -213,18 +297,7 @@ __global__ void __launch_bounds__(kSortThreads) k_bucket_dupcheck(const uint64_t
                 dup |= atomicAdd(&n_empty_key, 1u) > 0;
                 continue;
             }
-            // `second` is a hash output, so its low bits are a uniform slot; linear probing
-            // visits at most `size` slots and the table is at most 3/4 full.
-            uint32_t slot = (uint32_t)k & (size - 1);
-            for (uint32_t probe = 0; probe < size; ++probe) {
-                const uint64_t prev = atomicCAS((unsigned long long *)&tab[slot], kEmptyKey, k);
-                if (prev == kEmptyKey) break;
-                if (prev == k) {
-                    dup = true;
-                    break;
-                }
-                slot = (slot + 1) & (size - 1);
-            }
+            dup |= dup_insert(tab, size, k);
         }
         if (dup) set_error(status, RSB_ERR_DUPLICATE_KEY, b);
         __syncthreads();
@@ -387,7 +460,7 @@ void launch_hash_u64(const uint64_t *keys, uint64_t n, uint64_t *out128, cudaStr
 void launch_hash_strings(const uint8_t *bytes, const uint64_t *offsets, uint64_t n, uint64_t base, uint64_t *out128,
                          cudaStream_t st) {
     use_max_smem(k_hash_strings);
-    k_hash_strings<<<grid_for(n, 128, device_sm_count() * 32), 128, 0, st>>>(bytes, offsets, n, base, (ulonglong2 *)out128);
+    k_hash_strings<<<grid_for(n, kHashThreads, device_sm_count() * 32), kHashThreads, 0, st>>>(bytes, offsets, n, base, (ulonglong2 *)out128);
     count_launches(1);
 }
 

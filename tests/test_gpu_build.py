@@ -98,6 +98,43 @@ def test_string_keys_hash_like_oracle(rsb, oracle_mod, engine):
     assert np.array_equal(rsb.hash_strings((data, offsets), engine), oracle_mod.hash_strings(data, offsets))
 
 
+@pytest.mark.parametrize("shift", [0, 1, 7, 15, 16, 33])
+def test_string_hash_staging_paths(rsb, oracle_mod, engine, shift):
+    """Warps of 32 keys whose bytes fit the per-warp staging buffer hash from shared memory,
+    wider ones from global memory; both, at every start alignment (keys sliced `shift`
+    bytes into a larger buffer), give the oracle's hashes."""
+    rng = np.random.default_rng(100 + shift)
+    lens = np.concatenate([rng.integers(0, 64, 3000),           # staged warps
+                           rng.integers(60, 300, 200),          # warps wider than the buffer
+                           np.zeros(40, dtype=np.int64),        # empty keys
+                           rng.integers(0, 16, 1000)])          # short keys, one 16-byte block
+    offsets = np.zeros(lens.size + 1, dtype=np.uint64)
+    offsets[1:] = np.cumsum(lens)
+    body = rng.integers(0, 256, int(offsets[-1]), dtype=np.uint8)
+    data = np.concatenate([rng.integers(0, 256, shift, dtype=np.uint8), body,
+                           rng.integers(0, 256, 19, dtype=np.uint8)])
+    want = oracle_mod.hash_strings(body, offsets)
+    assert np.array_equal(rsb.hash_strings((data, offsets + np.uint64(shift)), engine), want)
+
+
+def test_evaluation_statistic_matches_seeds(rsb, oracle_mod, engine):
+    """The build's algorithmic evaluation count (used for the measured evaluation rates) is
+    the sum over nodes of (candidates up to the seed) x (node size), candidates being
+    rotation bases for full leaves."""
+    for leaf, b, n in ((8, 100, 50_000), (12, 1000, 30_000), (16, 2000, 10_000)):
+        keys = oracle_mod.keygen_hash128(SEED + 3 * leaf, n)
+        f = rsb.GPURecSplit(keys, bucket_size=b, leaf_size=leaf, engine=engine, keep_seeds=True)
+        seeds, sizes = f.seeds()
+        s = seeds.astype(object)
+        m = sizes.astype(object)
+        trials = [x // leaf + 1 if k == leaf else x + 1 for x, k in zip(s, m)]
+        want = sum(t * k for t, k in zip(trials, m))
+        st = f.stats()
+        assert st["evals_alg"] == want
+        assert sum(st["evals_stage"]) == want
+        f.close()
+
+
 def test_string_build_and_query(rsb, oracle_mod, engine):
     data, offsets = oracle_mod.keygen_strings(42, 50000)
     ref = oracle_mod.build_mphf(oracle_mod.hash_strings(data, offsets), 8, 100)
@@ -162,6 +199,31 @@ def test_duplicate_keys_rejected(rsb, oracle_mod, engine):
     # the engine stays usable
     f = rsb.GPURecSplit(keys[:3000], bucket_size=100, leaf_size=8, engine=engine)
     assert f.get_bits() > 0
+
+
+@pytest.mark.parametrize("b", [100, 1000, 2000])
+def test_duplicates_in_small_and_large_buckets(rsb, oracle_mod, engine, b):
+    """Buckets of at most 256 keys are checked by one warp each, larger ones by a CTA; both
+    find a repeated key, a repeated empty-slot marker (second half all ones) and nothing in
+    keys that only share a table slot."""
+    keys = oracle_mod.keygen_hash128(SEED + b, 20_000)
+    same_slot = keys.copy()
+    same_slot[5, 0] = same_slot[9, 0]                    # same bucket, second halves that
+    same_slot[5, 1] = same_slot[9, 1] ^ (1 << 40)        # differ only above the slot bits
+    f = rsb.GPURecSplit(same_slot, bucket_size=b, leaf_size=8, engine=engine)
+    assert f.serialize() == oracle_mod.build_mphf(same_slot, 8, b).bytes.tobytes()
+    one_marker = keys.copy()
+    one_marker[7, 1] = np.uint64(0xFFFFFFFFFFFFFFFF)
+    f = rsb.GPURecSplit(one_marker, bucket_size=b, leaf_size=8, engine=engine)
+    assert f.serialize() == oracle_mod.build_mphf(one_marker, 8, b).bytes.tobytes()
+    two_markers = one_marker.copy()
+    two_markers[11] = two_markers[7]
+    repeated = keys.copy()
+    repeated[19_000] = repeated[3]
+    for bad in (two_markers, repeated):
+        with pytest.raises(rsb.RSBError) as e:
+            rsb.GPURecSplit(bad, bucket_size=b, leaf_size=8, engine=engine)
+        assert e.value.name == "DUPLICATE_KEY"
 
 
 def test_oversized_bucket_rejected(rsb, oracle_mod, engine):
