@@ -186,7 +186,7 @@ class Engine:
     def set_schedule(self, leaf_size: int, stage: int, size_class: int, seeds_per_lane: int,
                      occupancy_pct: int = 100) -> None:
         """Schedule of one search stage (rsb_engine_set_schedule): 17/18 aggregation levels
-        (8, 12 or 16 seeds per lane), 19 rotation leaves (4, 8 or 12 bases per lane); size class
+        (4, 8, 12 or 16 seeds per lane), 19 rotation leaves (4, 8 or 12 bases per lane); size class
         0 below 2^20 keys, 1 from 2^20, 2 from 2^24. seeds_per_lane 0 restores the built-in schedule."""
         _check(lib().rsb_engine_set_schedule(self._h, leaf_size, stage, size_class, seeds_per_lane, occupancy_pct),
                "rsb_engine_set_schedule")

@@ -259,7 +259,7 @@ cudaError_t enqueue_searches(rsb_engine *e, const SearchCtx &sc, const LeafTable
         if ((err = cudaMemsetAsync(sc.slots, 0xFF, sc.nslots * sizeof(uint32_t), st)) != cudaSuccess) return err;
         const StageSchedule sa = engine_schedule(e, leaf, kStageLower, keys);
         const StageSchedule sl = engine_schedule(e, leaf, kStageLeafRot, keys);
-        const StageSchedule aggr{sa.seeds_per_lane == 8 ? 8 : 12, sa.occupancy_pct};
+        const StageSchedule aggr{sa.seeds_per_lane <= 8 ? 8 : 12, sa.occupancy_pct};
         const StageSchedule lf{sl.seeds_per_lane, 100};
         e->last_seeds_per_lane[kStageUpper] = e->last_seeds_per_lane[kStageLower] = aggr.seeds_per_lane;
         e->last_seeds_per_lane[kStageLeafRot] = lf.seeds_per_lane;

@@ -168,7 +168,7 @@ int schedule_size_class(uint64_t keys) { return keys >= (1ull << 24) ? 2 : keys 
 bool schedule_valid(int stage, const StageSchedule &s) {
     if (s.occupancy_pct < 1 || s.occupancy_pct > 100) return false;
     if (stage == kStageUpper || stage == kStageLower)
-        return s.seeds_per_lane == 8 || s.seeds_per_lane == 12 || s.seeds_per_lane == 16;
+        return s.seeds_per_lane == 4 || s.seeds_per_lane == 8 || s.seeds_per_lane == 12 || s.seeds_per_lane == 16;
     if (stage == kStageLeafRot) return s.seeds_per_lane == 4 || s.seeds_per_lane == 8 || s.seeds_per_lane == 12;
     return false;
 }

@@ -22,7 +22,7 @@ namespace {
 // multiply-add per key on a full node (two integer ops more on other nodes; moment_sums and
 // add_part) instead of a packed part count, and that
 // about 1 / (2.5 * sqrt(m * var(p))) of the seeds pass (1.9 % at m = 112, fanout 7).
-// Phase A applies it to every seed of a window (8, 12 or 16 per lane); the survivors go to a
+// Phase A applies it to every seed of a window (4, 8, 12 or 16 per lane); the survivors go to a
 // per-warp queue in shared memory, and phase B gives each lane one queued seed for the exact
 // part count, lowest seeds first, before the warp takes its next window (aggr_phase_b), so
 // every seed below the node's final best is fully checked and the minimum is unchanged.
@@ -659,6 +659,7 @@ void launch_aggr(const SearchCtx &c, const StageSchedule &s, cudaStream_t st) {
 template <int LEAF, int STAGE>
 void launch_aggr_s(const SearchCtx &c, const StageSchedule &s, cudaStream_t st) {
     switch (s.seeds_per_lane) {
+        case 4: launch_aggr<LEAF, STAGE, 4>(c, s, st); break;
         case 8: launch_aggr<LEAF, STAGE, 8>(c, s, st); break;
         case 16: launch_aggr<LEAF, STAGE, 16>(c, s, st); break;
         default: launch_aggr<LEAF, STAGE, 12>(c, s, st); break;

@@ -111,7 +111,7 @@ rsb_status rsb_engine_set_watchdog(rsb_engine *engine, double seconds);
  * constants are fixed, GPURecSplit.cuh:420-425): candidates per lane of a search window and
  * the percentage of the engine's occupancy the stage's grid keeps, for builds of `leaf_size`
  * in size class `size_class` (0: fewer than 2^20 keys, 1: 2^20 to 2^24, 2: at least 2^24).
- * `stage`: 17 upper aggregation (seeds_per_lane 8, 12 or 16), 18 lower aggregation (8, 12 or 16), 19 rotation
+ * `stage`: 17 upper aggregation (seeds_per_lane 4, 8, 12 or 16), 18 lower aggregation (4, 8, 12 or 16), 19 rotation
  * leaves (bases per lane 4, 8 or 12); occupancy 1..100. seeds_per_lane 0 restores the
  * built-in schedule (the table gpurecsplit_b200/tune.py measured). Every schedule finds the
  * same minimum seeds: results never change, only speed. */

@@ -9,7 +9,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-AGGR = (8, 12, 16)
+AGGR = (4, 8, 12, 16)
 LEAF = (4, 8, 12)
 
 
@@ -46,7 +46,7 @@ def test_schedule_arguments(rsb):
         lower0 = e.schedule(16, 18, 0)
         e.set_schedule(16, 17, 2, 16, 60)  # the entry of stage 17, class 2 is not stage 18's
         assert e.schedule(16, 17, 2) == (16, 60) and e.schedule(16, 18, 0) == lower0
-        for args in ((16, 18, 1, 4, 100), (16, 19, 1, 16, 100), (16, 18, 3, 8, 100), (16, 20, 0, 8, 100),
+        for args in ((16, 18, 1, 6, 100), (16, 19, 1, 16, 100), (16, 18, 3, 8, 100), (16, 20, 0, 8, 100),
                      (1, 18, 0, 8, 100), (16, 18, 0, 8, 0), (16, 18, 0, 8, 101)):
             with pytest.raises(rsb.RSBError) as err:
                 e.set_schedule(*args)
