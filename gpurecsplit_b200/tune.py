@@ -107,6 +107,14 @@ def measure(rsb, engine, leaf: int, size_class: int, n: int, repeats: int) -> di
     return times
 
 
+def choose(times_by_size: list) -> tuple:
+    """The schedule of one stage from its median times at one or more workload sizes
+    ([{(candidates, occupancy): ms}, ...], the same schedules at every size): the least summed
+    time relative to each size's fastest. Returns (schedule, {schedule: score})."""
+    score = {c: sum(t[c] / min(t.values()) for t in times_by_size) for c in times_by_size[0]}
+    return min(score, key=score.get), score
+
+
 def tune_one(rsb, engine, leaf: int, size_class: int, repeats: int, log) -> list:
     """Measures every candidate schedule for one (leaf, size class) at each of the class's
     sizes; returns table entries."""
@@ -116,8 +124,7 @@ def tune_one(rsb, engine, leaf: int, size_class: int, repeats: int, log) -> list
     for stage in STAGES:
         default = engine.schedule(leaf, stage, size_class)
         t = per_size[sizes[0]][stage]
-        score = {c: sum(per_size[n][stage][c] / min(per_size[n][stage].values()) for n in sizes) for c in t}
-        best = min(t, key=score.get)
+        best, score = choose([per_size[n][stage] for n in sizes])
         entry = {"leaf": leaf, "stage": stage, "size_class": size_class, "seeds_per_lane": best[0],
                  "occupancy_pct": best[1], "ms_best": round(t[best], 4), "ms_builtin": round(t.get(default, -1), 4),
                  "builtin": list(default), "keys": sizes[0], "bucket_size": bucket_size_for(leaf),

@@ -39,3 +39,15 @@ def test_table_matches_the_measurements():
             assert e["score"][chosen] <= min(e["score"].values()) + 1e-9
         else:
             assert e["ms_best"] <= min(e["ms"].values()) + 1e-9
+
+
+def test_tuner_choice_over_sizes():
+    """A schedule that wins narrowly at the small end of a size class but loses clearly at its
+    large end is not chosen; with one size the fastest is."""
+    from gpurecsplit_b200.tune import choose
+    small = {(4, 75): 0.0686, (12, 75): 0.0646, (8, 100): 0.0809}
+    large = {(4, 75): 0.2099, (12, 75): 0.2735, (8, 100): 0.2325}
+    best, score = choose([small, large])
+    assert best == (4, 75) and score[(4, 75)] < score[(12, 75)]
+    assert choose([small])[0] == (12, 75)
+    assert abs(choose([small])[1][(12, 75)] - 1.0) < 1e-12
