@@ -51,6 +51,31 @@ def test_equivalence_grid(rsb, oracle_mod, engine, leaf, b, n):
     assert np.array_equal(np.sort(q), np.arange(n, dtype=np.uint64))
 
 
+def _grid_other_buckets():
+    """The remaining bucket sizes of the reference's correctness grid (test/correctness.hpp:25),
+    with the same leaf-size limits as _grid."""
+    out = []
+    for leaf in range(2, 25):
+        for b in (3, 4, 6, 7, 8, 9, 75, 231, 1009, 1300):
+            if leaf >= 13 and b > 25:
+                continue
+            if leaf >= 19 and b > 10:
+                continue
+            for n in (100, 2000):
+                out.append((leaf, b, n))
+    return out
+
+
+@pytest.mark.parametrize("leaf,b,n", _grid_other_buckets())
+def test_equivalence_grid_other_buckets(rsb, oracle_mod, engine, leaf, b, n):
+    keys = oracle_mod.keygen_hash128(SEED ^ b, n)
+    ref, f = _build_both(rsb, oracle_mod, engine, keys, leaf, b)
+    seeds, sizes = f.seeds()
+    assert np.array_equal(sizes, ref.sizes)
+    assert np.array_equal(seeds, ref.seeds)
+    assert f.serialize() == ref.bytes.tobytes()
+
+
 @pytest.mark.parametrize("leaf,b,n", [(8, 100, 100000), (12, 1000, 30000), (16, 2000, 12000), (10, 483, 20000),
                                       (6, 25, 50000), (14, 75, 20000), (4, 1009, 20000), (20, 10, 5000)])
 def test_equivalence_larger(rsb, oracle_mod, engine, leaf, b, n):
